@@ -1,0 +1,646 @@
+// abi.cu -- the extern "C" entry points declared in include/ghc.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/ghc.h"
+#include "ghc_internal.h"
+#include "problem.h"
+
+namespace ghc {
+const char* last_error();
+int launch_f2d(const float* s, double* d, long long n, void* stream);
+int launch_debug_f(const uint8_t* conv, const double* t, const double* dt, float* dbg, long long n, void* stream);
+int launch_debug_d(const uint8_t* conv, const double* t, const double* dt, double* dbg, long long n, void* stream);
+int launch_diff_d(const double* s, const double* t, double* d, long long n_hyp, int P1, void* stream);
+}  // namespace ghc
+
+using namespace ghc;
+
+struct ghc_problem {
+  Problem pb;
+};
+
+namespace {
+
+int sm_count() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 1;
+}
+
+int cuda_fail(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return GHC_ERR_CUDA;
+}
+
+int track_code(int rc) {
+  if (rc == 0) return GHC_OK;
+  if (rc == -10) {
+    set_error("system size or kind has no compiled tracker (P2C N in {3,4,5,6,8,10,11,12,16,18}, PH N = 30)");
+    return GHC_ERR_RANGE;
+  }
+  if (rc == -11) {
+    set_error("unknown precision mode");
+    return GHC_ERR_ARG;
+  }
+  return cuda_fail("tracker launch");
+}
+
+TrackParams base_params(const Problem& pb) {
+  TrackParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.kind = pb.kind;
+  p.N = pb.N;
+  p.P = pb.P;
+  p.M = pb.M;
+  p.K = pb.K;
+  p.max_steps = pb.max_steps;
+  p.max_corr = pb.max_corr;
+  p.incr = pb.incr;
+  p.n_hx_terms = (int)pb.hx_terms.size();
+  p.n_ht_terms = (int)pb.ht_terms.size();
+  p.hx_terms = pb.dev.hx_terms;
+  p.hx_off = pb.dev.hx_off;
+  p.ht_terms = pb.dev.ht_terms;
+  p.ht_off = pb.dev.ht_off;
+  p.t_switch = 2.0;
+  return p;
+}
+
+PolishParams polish_params(const TrackParams& t, double* endpoints, const uint8_t* conv, double* resid, int iters) {
+  PolishParams q;
+  std::memset(&q, 0, sizeof(q));
+  q.kind = t.kind;
+  q.N = t.N;
+  q.P = t.P;
+  q.M = t.M;
+  q.K = t.K;
+  q.n_hx_terms = t.n_hx_terms;
+  q.n_ht_terms = t.n_ht_terms;
+  q.hx_terms = t.hx_terms;
+  q.hx_off = t.hx_off;
+  q.ht_terms = t.ht_terms;
+  q.ht_off = t.ht_off;
+  q.n_items = t.n_items;
+  q.paths_per_hyp = t.paths_per_hyp;
+  q.coef_hx = t.coef_hx;
+  q.stride_hx = t.stride_hx;
+  q.coef_ht = t.coef_ht;
+  q.stride_ht = t.stride_ht;
+  q.p_start = t.p_start;
+  q.p_tgt = t.p_tgt;
+  q.p_diff = t.p_diff;
+  q.stride_p = t.stride_p;
+  q.endpoints = endpoints;
+  q.ld = t.ld_out;
+  q.conv = conv;
+  q.resid = resid;
+  q.iters = iters;
+  return q;
+}
+
+// Pointer array of the reference layout: entry p == base + p * (N+1) complex.
+template <typename T>
+int regular_base(T* const* d_ptrs, long long n, int N, T** base) {
+  std::vector<T*> h((size_t)n);
+  if (cudaMemcpy(h.data(), d_ptrs, n * sizeof(T*), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return cuda_fail("copy of pointer array");
+  for (long long i = 0; i < n; ++i) {
+    if (h[i] != h[0] + 2 * i * (N + 1)) {
+      set_error("pointer array is not the reference's regular layout (base + p*(N+1))");
+      return GHC_ERR_LAYOUT;
+    }
+  }
+  *base = h[0];
+  return GHC_OK;
+}
+
+// Tables passed to a drop-in wrapper: the handle's compiled copy when they are
+// identical to the files it loaded, else compiled now into `tmp` device memory.
+int dropin_tables(Problem& pb, const int* d_hx, const int* d_ht, TrackParams& p, std::vector<void*>& tmp) {
+  std::vector<int32_t> hx(pb.hx_raw.size()), ht(pb.ht_raw.size());
+  if (cudaMemcpy(hx.data(), d_hx, hx.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(ht.data(), d_ht, ht.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return cuda_fail("copy of index tables");
+  if (hx == pb.hx_raw && ht == pb.ht_raw) return GHC_OK;
+  std::vector<uint64_t> hxt, htt;
+  std::vector<uint16_t> hxo, hto;
+  int rc = compile_tables(hx, ht, pb, hxt, hxo, htt, hto);
+  if (rc) return rc;
+  void *a, *b, *c, *d;
+  if (cudaMalloc(&a, std::max<size_t>(1, hxt.size()) * 8) || cudaMalloc(&b, hxo.size() * 2) ||
+      cudaMalloc(&c, std::max<size_t>(1, htt.size()) * 8) || cudaMalloc(&d, hto.size() * 2))
+    return cuda_fail("table upload");
+  tmp.insert(tmp.end(), {a, b, c, d});
+  cudaMemcpy(a, hxt.data(), hxt.size() * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(b, hxo.data(), hxo.size() * 2, cudaMemcpyHostToDevice);
+  cudaMemcpy(c, htt.data(), htt.size() * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(d, hto.data(), hto.size() * 2, cudaMemcpyHostToDevice);
+  p.hx_terms = (const uint64_t*)a;
+  p.hx_off = (const uint16_t*)b;
+  p.ht_terms = (const uint64_t*)c;
+  p.ht_off = (const uint16_t*)d;
+  p.n_hx_terms = (int)hxt.size();
+  p.n_ht_terms = (int)htt.size();
+  return GHC_OK;
+}
+
+struct TmpFree {
+  std::vector<void*> v;
+  ~TmpFree() {
+    for (void* p : v) cudaFree(p);
+  }
+};
+
+// Shared body of the four drop-in wrappers.  Real = float or double.
+template <typename Real>
+double dropin(const ghc_problem* h, void* stream, int max_steps, int max_corr, int incr, Real** d_start_arr,
+              Real** d_track_arr, const int* d_hx, const int* d_ht, const Real* coef_hx, const Real* coef_ht,
+              const Real* p_start, const Real* p_tgt, const Real* p_diff, uint8_t* d_conv, uint8_t* d_inf,
+              Real* d_debug) {
+  if (!h || !d_start_arr || !d_track_arr || !d_hx || !d_ht || !d_conv || !d_inf) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  Problem& pb = const_cast<Problem&>(h->pb);
+  int rc = ensure_device(pb);
+  if (rc) return rc;
+  const bool fp32 = std::is_same<Real, float>::value;
+  const long long n = pb.paths;
+  Real *start_base, *track_base;
+  if ((rc = regular_base(d_start_arr, n, pb.N, &start_base)) || (rc = regular_base(d_track_arr, n, pb.N, &track_base)))
+    return rc;
+  TrackParams p = base_params(pb);
+  TmpFree tmp;
+  if ((rc = dropin_tables(pb, d_hx, d_ht, p, tmp.v))) return rc;
+  p.max_steps = max_steps;
+  p.max_corr = max_corr;
+  p.incr = incr;
+  p.n_items = n;
+  p.paths_per_hyp = pb.paths;
+  p.start_sols = start_base;
+  p.ld_start = pb.N + 1;
+  p.track_in = track_base;
+  p.ld_track = pb.N + 1;
+  p.endpoints = track_base;
+  p.ld_out = pb.N + 1;
+  // scratch: double copies of coefficient/parameter tables + t/dt
+  const long long nhx = pb.kind == KIND_P2C ? 2LL * (pb.M + 1) * (pb.K + 1) : 0;
+  const long long nht = pb.kind == KIND_P2C ? 2LL * (pb.M + 1) * pb.K : 0;
+  const long long npar = pb.kind == KIND_PH ? 2LL * (pb.P + 1) : 0;
+  const size_t bytes = sizeof(double) * (size_t)(nhx + nht + 3 * npar + 2 * n) + 256;
+  double* s = (double*)scratch(pb, bytes);
+  if (!s) return cuda_fail("scratch allocation");
+  double* d_chx = s;
+  double* d_cht = d_chx + nhx;
+  double* d_ps = d_cht + nht;
+  double* d_pt = d_ps + npar;
+  double* d_pd = d_pt + npar;
+  double* d_t = d_pd + npar;
+  double* d_dt = d_t + n;
+  cudaStream_t st = (cudaStream_t)stream;
+  auto to_double = [&](const Real* src, double* dst, long long cnt) -> int {
+    if (cnt <= 0) return 0;
+    if (fp32) return launch_f2d((const float*)src, dst, cnt, stream);
+    return cudaMemcpyAsync(dst, src, cnt * sizeof(double), cudaMemcpyDeviceToDevice, st) == cudaSuccess ? 0 : -1;
+  };
+  if (pb.kind == KIND_P2C) {
+    if (!coef_hx || !coef_ht) {
+      set_error("null coefficient table");
+      return GHC_ERR_ARG;
+    }
+    if (to_double(coef_hx, d_chx, nhx) || to_double(coef_ht, d_cht, nht)) return cuda_fail("coefficient copy");
+    p.coef_hx = d_chx;
+    p.coef_ht = d_cht;
+  } else {
+    if (!p_start || !p_tgt || !p_diff) {
+      set_error("null parameter array");
+      return GHC_ERR_ARG;
+    }
+    if (to_double(p_start, d_ps, npar) || to_double(p_tgt, d_pt, npar) || to_double(p_diff, d_pd, npar))
+      return cuda_fail("parameter copy");
+    p.p_start = d_ps;
+    p.p_tgt = d_pt;
+    p.p_diff = d_pd;
+  }
+  p.conv = d_conv;
+  p.infy = d_inf;
+  p.t_end = d_t;
+  p.dt_end = d_dt;
+  p.counter = pb.dev.counter;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  rc = track_code(launch_track(p, fp32 ? PREC_FP32 : PREC_FP64, stream, sm_count()));
+  cudaEventRecord(e1, st);
+  if (!rc && d_debug) {
+    if (fp32) rc = launch_debug_f(d_conv, d_t, d_dt, (float*)d_debug, n, stream);
+    else rc = launch_debug_d(d_conv, d_t, d_dt, (double*)d_debug, n, stream);
+    if (rc) rc = cuda_fail("debug output");
+  }
+  float ms = 0;
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = cuda_fail("tracker execution");
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  return ms * 1e-3;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ghc_last_error(void) { return ghc::last_error(); }
+int ghc_version(void) { return 1; }
+
+int ghc_problem_load(const char* root, const char* name, ghc_problem** out) {
+  if (!root || !name || !out) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  std::unique_ptr<ghc_problem> h(new ghc_problem());
+  const int rc = load_problem(root, name, h->pb);
+  if (rc) return rc;
+  *out = h.release();
+  return GHC_OK;
+}
+
+void ghc_problem_free(ghc_problem* pb) { delete pb; }
+
+int ghc_problem_get_info(const ghc_problem* h, ghc_problem_info* info) {
+  if (!h || !info) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  const Problem& pb = h->pb;
+  std::memset(info, 0, sizeof(*info));
+  std::strncpy(info->name, pb.name.c_str(), sizeof(info->name) - 1);
+  info->kind = pb.kind;
+  info->N = pb.N;
+  info->P = pb.P;
+  info->M = pb.M;
+  info->K = pb.K;
+  info->paths = pb.paths;
+  info->Tx = pb.Tx;
+  info->Px = pb.Px;
+  info->Tt = pb.Tt;
+  info->Pt = pb.Pt;
+  info->max_steps = pb.max_steps;
+  info->max_corr = pb.max_corr;
+  info->incr_steps = pb.incr;
+  info->n_hx_terms = (int)pb.hx_terms.size();
+  info->n_ht_terms = (int)pb.ht_terms.size();
+  info->has_p2c_terms = pb.has_terms ? 1 : 0;
+  info->subwarp = track_subwarp_width(pb.N);
+  return GHC_OK;
+}
+
+int ghc_problem_start_sols(const ghc_problem* h, double* out) {
+  if (!h || !out) return GHC_ERR_ARG;
+  std::memcpy(out, h->pb.start_sols.data(), h->pb.start_sols.size() * sizeof(double));
+  return GHC_OK;
+}
+
+int ghc_problem_params(const ghc_problem* h, double* start, double* target) {
+  if (!h) return GHC_ERR_ARG;
+  if (start) std::memcpy(start, h->pb.start_params.data(), h->pb.start_params.size() * sizeof(double));
+  if (target) std::memcpy(target, h->pb.target_params.data(), h->pb.target_params.size() * sizeof(double));
+  return GHC_OK;
+}
+
+int ghc_problem_raw_tables(const ghc_problem* h, int32_t* hx, int32_t* ht) {
+  if (!h) return GHC_ERR_ARG;
+  if (hx) std::memcpy(hx, h->pb.hx_raw.data(), h->pb.hx_raw.size() * 4);
+  if (ht) std::memcpy(ht, h->pb.ht_raw.data(), h->pb.ht_raw.size() * 4);
+  return GHC_OK;
+}
+
+int ghc_p2c(const ghc_problem* h, const double* start, const double* target, double* hx, double* ht, int exact_ht) {
+  if (!h || !start || !target || !hx || !ht) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  return p2c_host(h->pb, start, target, hx, ht, exact_ht);
+}
+
+int ghc_p2c_device(const ghc_problem* h, int64_t n_hyp, const double* d_start, const double* d_targets, double* d_hx,
+                   double* d_ht, int exact_ht, void* stream) {
+  if (!h || !d_start || !d_targets || !d_hx || !d_ht || n_hyp < 0) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  Problem& pb = const_cast<Problem&>(h->pb);
+  if (pb.kind != KIND_P2C || !pb.has_terms) {
+    set_error("problem has no coefficient expressions (p2c_terms.txt)");
+    return GHC_ERR_NOP2C;
+  }
+  int rc = ensure_device(pb);
+  if (rc) return rc;
+  P2CParams p;
+  p.M = pb.M;
+  p.K = pb.K;
+  p.P = pb.P;
+  p.n_terms = (int)pb.p2c.size();
+  p.term_k = pb.dev.t_k;
+  p.term_coef = pb.dev.t_coef;
+  p.term_nf = pb.dev.t_nf;
+  p.term_fac_off = pb.dev.t_fac_off;
+  p.term_fac = pb.dev.t_fac;
+  p.k_off = pb.dev.k_off;
+  p.n_hyp = n_hyp;
+  p.p_start = d_start;
+  p.p_tgt = d_targets;
+  p.coef_hx = d_hx;
+  p.coef_ht = d_ht;
+  p.exact_ht = exact_ht;
+  rc = launch_p2c(p, stream);
+  if (rc == -10) {
+    set_error("Max_Order_Of_T above 8");
+    return GHC_ERR_RANGE;
+  }
+  return rc ? cuda_fail("p2c launch") : GHC_OK;
+}
+
+int ghc_track(const ghc_problem* h, const ghc_track_args* a, void* stream) {
+  if (!h || !a || !a->d_start_sols || !a->d_endpoints || !a->d_counter || a->n_hyp < 0) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  Problem& pb = const_cast<Problem&>(h->pb);
+  int rc = ensure_device(pb);
+  if (rc) return rc;
+  TrackParams p = base_params(pb);
+  if (a->max_steps > 0) p.max_steps = a->max_steps;
+  if (a->max_corr > 0) p.max_corr = a->max_corr;
+  if (a->incr_steps > 0) p.incr = a->incr_steps;
+  p.n_items = a->n_hyp * (long long)pb.paths;
+  p.paths_per_hyp = pb.paths;
+  p.start_sols = a->d_start_sols;
+  p.ld_start = pb.N;
+  p.track_in = nullptr;
+  p.ld_track = pb.N;
+  if (pb.kind == KIND_P2C) {
+    if (!a->d_coef_hx || !a->d_coef_ht) {
+      set_error("P2C problem needs d_coef_hx / d_coef_ht");
+      return GHC_ERR_ARG;
+    }
+    p.coef_hx = a->d_coef_hx;
+    p.coef_ht = a->d_coef_ht;
+    p.stride_hx = (long long)(pb.M + 1) * (pb.K + 1);
+    p.stride_ht = (long long)(pb.M + 1) * pb.K;
+  } else {
+    if (!a->d_p_start || !a->d_p_target || !a->d_p_diff) {
+      set_error("PH problem needs d_p_start / d_p_target / d_p_diff");
+      return GHC_ERR_ARG;
+    }
+    p.p_start = a->d_p_start;
+    p.p_tgt = a->d_p_target;
+    p.p_diff = a->d_p_diff;
+    p.stride_p = pb.P + 1;
+  }
+  p.endpoints = a->d_endpoints;
+  p.ld_out = pb.N;
+  p.status = a->d_status;
+  p.conv = a->d_conv;
+  p.infy = a->d_inf;
+  p.steps = a->d_steps;
+  p.corr = a->d_corr;
+  p.t_end = a->d_t_end;
+  p.dt_end = a->d_dt_end;
+  p.counter = a->d_counter;
+  p.t_switch = a->t_switch;
+  if (a->precision == GHC_PREC_FP64) p.t_switch = 2.0;
+  rc = track_code(launch_track(p, a->precision, stream, sm_count()));
+  if (rc) return rc;
+  const bool fp64_state = a->precision == GHC_PREC_FP64 || a->precision == GHC_PREC_MIXED;
+  if ((a->polish_iters > 0 || a->d_resid) && fp64_state) {
+    if (!a->d_conv) {
+      set_error("polish needs d_conv");
+      return GHC_ERR_ARG;
+    }
+    PolishParams q = polish_params(p, (double*)a->d_endpoints, a->d_conv, a->d_resid, a->polish_iters);
+    rc = launch_polish(q, stream);
+    if (rc) return track_code(rc);
+  }
+  return GHC_OK;
+}
+
+int ghc_count_results(int32_t N, int32_t paths, const double* z, const uint8_t* conv, const uint8_t* inf,
+                      double imag_tol, double dup_tol, ghc_counts* out) {
+  if (N < 1 || paths < 0 || !z || !conv || !inf || !out) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  // Evaluations::Evaluate_GPUHC_Sols (Evaluations.cpp:88-110)
+  ghc_counts c = {0, 0, 0, 0};
+  for (int bs = 0; bs < paths; ++bs) {
+    if (conv[bs]) ++c.converged;
+    if (inf[bs]) ++c.infinity;
+    if (conv[bs]) {
+      int nreal = 0;
+      for (int v = 0; v < N; ++v)
+        if (std::fabs(z[2 * ((size_t)bs * N + v) + 1]) <= imag_tol) ++nreal;
+      if (nreal == N) ++c.real;
+    }
+  }
+  // Evaluations::Find_Unique_Sols (Evaluations.cpp:127-176): the skip set is
+  // replaced (not merged) by each new duplicate set; members of a duplicate
+  // cluster are not counted.
+  std::set<int> skip, dup;
+  for (int bs = 0; bs < paths; ++bs) {
+    if (!conv[bs]) continue;
+    if (!skip.empty()) {
+      if (skip.count(bs)) continue;
+      dup.clear();
+    }
+    for (int ds = bs + 1; ds < paths; ++ds) {
+      int same = 0;
+      for (int v = 0; v < N; ++v) {
+        const double* a = z + 2 * ((size_t)bs * N + v);
+        const double* b = z + 2 * ((size_t)ds * N + v);
+        if (std::fabs(a[0] - b[0]) < dup_tol && std::fabs(a[1] - b[1]) < dup_tol) ++same;
+      }
+      if (same == N) dup.insert(ds);
+    }
+    if (dup.empty()) ++c.unique;
+    else skip = dup;
+  }
+  *out = c;
+  return GHC_OK;
+}
+
+double ghc_kernel_HC_Solver_P2C(const ghc_problem* pb, void* stream, int max_steps, int max_corr, int incr,
+                                float** d_startSols_array, float** d_Track_array, const int* d_Hx_idx,
+                                const int* d_Ht_idx, const float* d_phc_coeffs_Hx, const float* d_phc_coeffs_Ht,
+                                uint8_t* d_conv, uint8_t* d_inf, float* d_debug) {
+  if (pb && pb->pb.kind != KIND_P2C) {
+    set_error("not a P2C problem");
+    return GHC_ERR_ARG;
+  }
+  return dropin<float>(pb, stream, max_steps, max_corr, incr, d_startSols_array, d_Track_array, d_Hx_idx, d_Ht_idx,
+                       d_phc_coeffs_Hx, d_phc_coeffs_Ht, nullptr, nullptr, nullptr, d_conv, d_inf, d_debug);
+}
+
+double ghc_kernel_HC_Solver_P2C_z(const ghc_problem* pb, void* stream, int max_steps, int max_corr, int incr,
+                                  double** d_startSols_array, double** d_Track_array, const int* d_Hx_idx,
+                                  const int* d_Ht_idx, const double* d_phc_coeffs_Hx,
+                                  const double* d_phc_coeffs_Ht, uint8_t* d_conv, uint8_t* d_inf,
+                                  double* d_debug) {
+  if (pb && pb->pb.kind != KIND_P2C) {
+    set_error("not a P2C problem");
+    return GHC_ERR_ARG;
+  }
+  return dropin<double>(pb, stream, max_steps, max_corr, incr, d_startSols_array, d_Track_array, d_Hx_idx, d_Ht_idx,
+                        d_phc_coeffs_Hx, d_phc_coeffs_Ht, nullptr, nullptr, nullptr, d_conv, d_inf, d_debug);
+}
+
+double ghc_kernel_HC_Solver_PH(const ghc_problem* pb, void* stream, int max_steps, int max_corr, int incr,
+                               float** d_startSols_array, float** d_Track_array, const float* d_startParams,
+                               const float* d_targetParams, const float* d_diffParams, const int* d_Hx_idx,
+                               const int* d_Ht_idx, uint8_t* d_conv, uint8_t* d_inf, float* d_debug) {
+  if (pb && pb->pb.kind != KIND_PH) {
+    set_error("not a PH problem");
+    return GHC_ERR_ARG;
+  }
+  return dropin<float>(pb, stream, max_steps, max_corr, incr, d_startSols_array, d_Track_array, d_Hx_idx, d_Ht_idx,
+                       nullptr, nullptr, d_startParams, d_targetParams, d_diffParams, d_conv, d_inf, d_debug);
+}
+
+double ghc_kernel_HC_Solver_PH_z(const ghc_problem* pb, void* stream, int max_steps, int max_corr, int incr,
+                                 double** d_startSols_array, double** d_Track_array, const double* d_startParams,
+                                 const double* d_targetParams, const double* d_diffParams, const int* d_Hx_idx,
+                                 const int* d_Ht_idx, uint8_t* d_conv, uint8_t* d_inf, double* d_debug) {
+  if (pb && pb->pb.kind != KIND_PH) {
+    set_error("not a PH problem");
+    return GHC_ERR_ARG;
+  }
+  return dropin<double>(pb, stream, max_steps, max_corr, incr, d_startSols_array, d_Track_array, d_Hx_idx, d_Ht_idx,
+                        nullptr, nullptr, d_startParams, d_targetParams, d_diffParams, d_conv, d_inf, d_debug);
+}
+
+int ghc_solve_host(const ghc_problem* h, int32_t precision, int64_t n_hyp, const double* h_targets, double t_switch,
+                   int32_t polish_iters, double* h_endpoints, uint8_t* h_status, uint8_t* h_conv, uint8_t* h_inf,
+                   int32_t* h_steps, double* h_ms) {
+  if (!h || !h_endpoints || n_hyp < 1) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  if (precision != GHC_PREC_FP64 && precision != GHC_PREC_FP32 && precision != GHC_PREC_MIXED) {
+    set_error("unknown precision mode");
+    return GHC_ERR_ARG;
+  }
+  Problem& pb = const_cast<Problem&>(h->pb);
+  if (!h_targets) n_hyp = 1;
+  int rc = ensure_device(pb);
+  if (rc) return rc;
+  const bool fp32 = precision == GHC_PREC_FP32;
+  const long long n = n_hyp * (long long)pb.paths;
+  const int N = pb.N, P1 = pb.P + 1;
+  const size_t rs = fp32 ? sizeof(float) : sizeof(double);
+  const long long nhx = 2LL * (pb.M + 1) * (pb.K + 1), nht = 2LL * (pb.M + 1) * pb.K;
+  TmpFree tmp;
+  auto dmalloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
+    tmp.v.push_back(p);
+    return p;
+  };
+  void* d_start = dmalloc(2 * (size_t)pb.paths * N * rs);
+  double* d_ps = (double*)dmalloc(2 * (size_t)P1 * sizeof(double));
+  double* d_tg = (double*)dmalloc(2 * (size_t)P1 * n_hyp * sizeof(double));
+  double* d_pd = (double*)dmalloc(2 * (size_t)P1 * n_hyp * sizeof(double));
+  double* d_hx = pb.kind == KIND_P2C ? (double*)dmalloc(nhx * n_hyp * sizeof(double)) : nullptr;
+  double* d_ht = pb.kind == KIND_P2C ? (double*)dmalloc(std::max(nht, 1LL) * n_hyp * sizeof(double)) : nullptr;
+  void* d_ep = dmalloc(2 * (size_t)n * N * rs);
+  uint8_t* d_flags = (uint8_t*)dmalloc(3 * (size_t)n);
+  int32_t* d_steps = (int32_t*)dmalloc((size_t)n * 4 + 16);
+  if (!d_start || !d_ps || !d_tg || !d_pd || !d_ep || !d_flags || !d_steps ||
+      (pb.kind == KIND_P2C && (!d_hx || !d_ht)))
+    return cuda_fail("allocation");
+  if (pb.kind == KIND_P2C && !pb.has_terms) {
+    set_error("problem has no coefficient expressions (p2c_terms.txt)");
+    return GHC_ERR_NOP2C;
+  }
+  cudaStream_t st = 0;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) cudaEventCreate(&e);
+  std::vector<float> sf;
+  cudaEventRecord(ev[0], st);
+  if (fp32) {
+    sf.resize(pb.start_sols.size());
+    for (size_t i = 0; i < sf.size(); ++i) sf[i] = (float)pb.start_sols[i];
+    cudaMemcpyAsync(d_start, sf.data(), sf.size() * 4, cudaMemcpyHostToDevice, st);
+  } else {
+    cudaMemcpyAsync(d_start, pb.start_sols.data(), pb.start_sols.size() * 8, cudaMemcpyHostToDevice, st);
+  }
+  cudaMemcpyAsync(d_ps, pb.start_params.data(), 2 * (size_t)P1 * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_tg, h_targets ? h_targets : pb.target_params.data(), 2 * (size_t)P1 * n_hyp * 8,
+                  cudaMemcpyHostToDevice, st);
+  cudaEventRecord(ev[1], st);
+  if (pb.kind == KIND_P2C) {
+    rc = ghc_p2c_device(h, n_hyp, d_ps, d_tg, d_hx, d_ht, 0, st);
+  } else {
+    rc = launch_diff_d(d_ps, d_tg, d_pd, n_hyp, P1, st) ? cuda_fail("diff") : GHC_OK;
+  }
+  ghc_track_args a;
+  std::memset(&a, 0, sizeof(a));
+  a.n_hyp = n_hyp;
+  a.precision = precision;
+  a.t_switch = t_switch;
+  a.polish_iters = polish_iters;
+  a.d_start_sols = d_start;
+  a.d_coef_hx = d_hx;
+  a.d_coef_ht = d_ht;
+  a.d_p_start = d_ps;
+  a.d_p_target = d_tg;
+  a.d_p_diff = d_pd;
+  a.d_endpoints = d_ep;
+  a.d_status = d_flags;
+  a.d_conv = d_flags + n;
+  a.d_inf = d_flags + 2 * n;
+  a.d_steps = d_steps;
+  a.d_counter = pb.dev.counter;
+  if (!rc) rc = ghc_track(h, &a, st);
+  cudaEventRecord(ev[2], st);
+  std::vector<float> ef;
+  if (!rc) {
+    if (fp32) {
+      ef.resize(2 * (size_t)n * N);
+      cudaMemcpyAsync(ef.data(), d_ep, ef.size() * 4, cudaMemcpyDeviceToHost, st);
+    } else {
+      cudaMemcpyAsync(h_endpoints, d_ep, 2 * (size_t)n * N * 8, cudaMemcpyDeviceToHost, st);
+    }
+    if (h_status) cudaMemcpyAsync(h_status, d_flags, n, cudaMemcpyDeviceToHost, st);
+    if (h_conv) cudaMemcpyAsync(h_conv, d_flags + n, n, cudaMemcpyDeviceToHost, st);
+    if (h_inf) cudaMemcpyAsync(h_inf, d_flags + 2 * n, n, cudaMemcpyDeviceToHost, st);
+    if (h_steps) cudaMemcpyAsync(h_steps, d_steps, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+  }
+  cudaEventRecord(ev[3], st);
+  if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = cuda_fail("solve");
+  if (!rc && fp32)
+    for (size_t i = 0; i < ef.size(); ++i) h_endpoints[i] = ef[i];
+  if (h_ms) {
+    float m = 0;
+    cudaEventElapsedTime(&m, ev[0], ev[1]);
+    h_ms[0] = m;
+    cudaEventElapsedTime(&m, ev[1], ev[2]);
+    h_ms[1] = m;
+    cudaEventElapsedTime(&m, ev[2], ev[3]);
+    h_ms[2] = m;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,131 @@
+// ghc_internal.h -- definitions shared by the host library and the CUDA tracker.
+//
+// Problem layout (reference, GPU-HC/magmaHC/GPU_HC_Solver.cpp:44-83):
+//   N unknowns, P parameters, M unique coefficients (P2C), K = max order of t,
+//   dHdx table [N][N][Tx][Px], dHdt table [N][Tt][Pt]   (P2C, row-major)
+//   dHdx table [N*Tx*Px][N],   dHdt table [Tt*Pt][N]     (PH, transposed)
+//
+// The device never walks the raw tables.  The host compiles them once into
+// "terms": one 64-bit word per non-padding monomial term, grouped by Jacobian
+// entry (row, col) for H_x and by row for H / H_t, with CSR offsets.
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define GHC_HD __host__ __device__
+#else
+#define GHC_HD
+#endif
+
+namespace ghc {
+
+enum Kind : int { KIND_P2C = 0, KIND_PH = 1 };
+enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1, PREC_MIXED = 2 };
+enum Status : int { ST_CONVERGED = 0, ST_DIVERGED = 1, ST_STEP_CAP = 2 };
+
+constexpr int kMaxN = 32;
+constexpr int kMaxVarsPerTerm = 8;
+
+// term word layout
+//   bits  0.. 7  integer scale (int8)
+//   bits  8..10  number of variable factors nv (slot N, the constant 1, dropped)
+//   bits 11..20  P2C: coefficient index k (0..1023)
+//   bits 11..16  PH : parameter index a ; bits 17..22 PH: parameter index b
+//   bits 24..63  variable indices, 5 bits each, table order
+GHC_HD inline int term_scale(uint64_t w) { return (int)(int8_t)(w & 0xffu); }
+GHC_HD inline int term_nv(uint64_t w) { return (int)((w >> 8) & 7u); }
+GHC_HD inline int term_coef(uint64_t w) { return (int)((w >> 11) & 0x3ffu); }
+GHC_HD inline int term_pa(uint64_t w) { return (int)((w >> 11) & 0x3fu); }
+GHC_HD inline int term_pb(uint64_t w) { return (int)((w >> 17) & 0x3fu); }
+GHC_HD inline int term_var(uint64_t w, int q) { return (int)((w >> (24 + 5 * q)) & 31u); }
+
+// Everything the tracker kernel needs, by value.
+struct TrackParams {
+  // problem
+  int kind, N, P, M, K;
+  int max_steps, max_corr, incr;
+  int n_hx_terms, n_ht_terms;
+  const uint64_t* hx_terms;   // device
+  const uint16_t* hx_off;     // device [N*N+1]
+  const uint64_t* ht_terms;   // device
+  const uint16_t* ht_off;     // device [N+1]
+  // work items: item i = hypothesis i / paths_per_hyp, start path i % paths_per_hyp
+  long long n_items;
+  int paths_per_hyp;
+  // inputs (complex arrays interleaved re,im; state precision RS for sols)
+  const void* start_sols;  // [paths_per_hyp][ld_start]
+  int ld_start;
+  const void* track_in;    // optional initial track [n_items][ld_track] (nullptr -> start_sols)
+  int ld_track;
+  const double* coef_hx;   // P2C [n_hyp][(M+1)(K+1)] complex double
+  long long stride_hx;     // in complex entries (0 -> shared by all hypotheses)
+  const double* coef_ht;   // P2C [n_hyp][(M+1)K]
+  long long stride_ht;
+  const double* p_start;   // PH [P+1]
+  const double* p_tgt;     // PH [n_hyp][P+1]
+  const double* p_diff;    // PH [n_hyp][P+1]
+  long long stride_p;
+  // outputs
+  void* endpoints;         // [n_items][ld_out] complex RS
+  int ld_out;
+  uint8_t* status;
+  uint8_t* conv;
+  uint8_t* infy;
+  int* steps;
+  int* corr;
+  double* t_end;
+  double* dt_end;
+  // scratch
+  int* counter;            // one int, zero before launch
+  // mixed precision: corrector in the high precision once t >= t_switch
+  double t_switch;
+};
+
+struct PolishParams {
+  int kind, N, P, M, K;
+  int n_hx_terms, n_ht_terms;
+  const uint64_t* hx_terms;
+  const uint16_t* hx_off;
+  const uint64_t* ht_terms;
+  const uint16_t* ht_off;
+  long long n_items;
+  int paths_per_hyp;
+  const double* coef_hx;
+  long long stride_hx;
+  const double* coef_ht;
+  long long stride_ht;
+  const double* p_start;
+  const double* p_tgt;
+  const double* p_diff;
+  long long stride_p;
+  double* endpoints;  // [n_items][ld] complex double, in/out
+  int ld;
+  const uint8_t* conv;
+  double* resid;      // [n_items] |H(x,1)| after polish, -1 when not converged
+  int iters;
+};
+
+struct P2CParams {
+  int M, K, P;
+  int n_terms;
+  const int* term_k;        // [n_terms]
+  const double* term_coef;  // [n_terms]
+  const int* term_nf;       // [n_terms]
+  const int* term_fac_off;  // [n_terms+1]
+  const int* term_fac;      // factors (param indices)
+  const int* k_off;         // [M+1] term ranges per coefficient
+  long long n_hyp;
+  const double* p_start;    // [P+1] complex
+  const double* p_tgt;      // [n_hyp][P+1] complex
+  double* coef_hx;          // [n_hyp][(M+1)(K+1)]
+  double* coef_ht;          // [n_hyp][(M+1)K]
+  int exact_ht;
+};
+
+// launch entry points implemented in tracker.cu / p2c.cu
+int launch_track(const TrackParams& p, int precision, void* stream, int n_sm);
+int launch_polish(const PolishParams& p, void* stream);
+int launch_p2c(const P2CParams& p, void* stream);
+int track_subwarp_width(int N);
+
+}  // namespace ghc

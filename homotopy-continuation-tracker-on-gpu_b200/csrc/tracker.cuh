@@ -1,0 +1,621 @@
+// tracker.cuh -- the homotopy path tracker for sm_100a.
+//
+// One sub-warp of W lanes (W = next power of two >= N, at least 4) tracks one
+// path: lane r owns equation row r (its row of H_x lives in registers) and
+// component r of the track.  The 32/W sub-warps of a warp run in lockstep
+// through one warp-uniform loop (one path step per trip), so every shuffle and
+// __syncwarp sees the full warp; a sub-warp whose path ends writes its
+// endpoint and takes the next path from a global counter (work stealing).
+//
+// Per path step (reference GPU-HC/magmaHC/gpu-kernels/kernel_HC_Solver_P3P.cu:115-254,
+// PH variant kernel_HC_Solver_trifocal_2op1p_30x30.cu:155-301):
+//   end-zone clamp -> 4 RK stages (coefficients c_k(t) -> H_x, -H_t -> LU solve)
+//   -> Newton corrector (H_x, H -> LU solve, success/infinity tests) -> step control.
+//
+// Arithmetic follows the oracle's operation order exactly (explicit fma,
+// *_rn intrinsics so nothing else is contracted), so the FP64 tracker matches
+// the oracle bit for bit.  Index tables are pre-compiled into term words
+// (ghc_internal.h) and staged once per CTA in shared memory.
+#pragma once
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include <cstdint>
+#include <type_traits>
+
+#include "ghc_internal.h"
+
+namespace ghc {
+namespace dev {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename R>
+struct cx {
+  R re, im;
+};
+
+__device__ __forceinline__ double f_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float f_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double f_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float f_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double f_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float f_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double f_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float f_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double f_div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float f_div(float a, float b) { return __fdiv_rn(a, b); }
+
+template <typename R>
+__device__ __forceinline__ cx<R> mk(R a, R b) {
+  cx<R> r;
+  r.re = a;
+  r.im = b;
+  return r;
+}
+template <typename R>
+__device__ __forceinline__ cx<R> c_add(cx<R> a, cx<R> b) {
+  return mk(f_add(a.re, b.re), f_add(a.im, b.im));
+}
+template <typename R>
+__device__ __forceinline__ cx<R> c_sub(cx<R> a, cx<R> b) {
+  return mk(f_sub(a.re, b.re), f_sub(a.im, b.im));
+}
+template <typename R>
+__device__ __forceinline__ cx<R> c_scale(R s, cx<R> a) {
+  return mk(f_mul(s, a.re), f_mul(s, a.im));
+}
+// a*b
+template <typename R>
+__device__ __forceinline__ cx<R> c_mul(cx<R> a, cx<R> b) {
+  return mk(f_fma(a.re, b.re, -f_mul(a.im, b.im)), f_fma(a.re, b.im, f_mul(a.im, b.re)));
+}
+// c + a*b
+template <typename R>
+__device__ __forceinline__ cx<R> c_fma(cx<R> a, cx<R> b, cx<R> c) {
+  return mk(f_fma(a.re, b.re, f_fma(-a.im, b.im, c.re)), f_fma(a.re, b.im, f_fma(a.im, b.re, c.im)));
+}
+// c - a*b
+template <typename R>
+__device__ __forceinline__ cx<R> c_fnma(cx<R> a, cx<R> b, cx<R> c) {
+  return mk(f_fma(-a.re, b.re, f_fma(a.im, b.im, c.re)), f_fma(-a.re, b.im, f_fma(-a.im, b.re, c.im)));
+}
+// 1/b, Smith (1962) with one reciprocal of the scaled denominator
+template <typename R>
+__device__ __forceinline__ cx<R> c_rcp(cx<R> b) {
+  if (fabs(b.re) >= fabs(b.im)) {
+    const R r = f_div(b.im, b.re);
+    const R d = f_fma(b.im, r, b.re);
+    const R inv = f_div(R(1), d);
+    return mk(inv, -f_mul(r, inv));
+  } else {
+    const R r = f_div(b.re, b.im);
+    const R d = f_fma(b.re, r, b.im);
+    const R inv = f_div(R(1), d);
+    return mk(f_mul(r, inv), -inv);
+  }
+}
+template <typename R>
+__device__ __forceinline__ R c_abs2(cx<R> a) {
+  return f_fma(a.re, a.re, f_mul(a.im, a.im));
+}
+template <typename R, typename S>
+__device__ __forceinline__ cx<R> c_cast(cx<S> a) {
+  return mk((R)a.re, (R)a.im);
+}
+
+__device__ __forceinline__ double shfl_xor(double v, int off, int w) { return __shfl_xor_sync(kFull, v, off, w); }
+__device__ __forceinline__ float shfl_xor(float v, int off, int w) { return __shfl_xor_sync(kFull, v, off, w); }
+
+// compiled tables staged in shared memory
+struct Tables {
+  const uint64_t* hx_terms;
+  const uint16_t* hx_off;
+  const uint64_t* ht_terms;
+  const uint16_t* ht_off;
+};
+
+// acc += p * x[v0] * x[v1] ...  (reference monomial term, slot N dropped)
+template <typename R>
+__device__ __forceinline__ cx<R> acc_term(cx<R> acc, cx<R> p, uint64_t w, const cx<R>* xs) {
+  const int nv = term_nv(w);
+  if (nv == 0) return c_add(acc, p);
+  for (int q = 0; q < nv - 1; ++q) p = c_mul(p, xs[term_var(w, q)]);
+  return c_fma(p, xs[term_var(w, nv - 1)], acc);
+}
+
+// c_k(t), c'_k(t) for k = l, l+W, ... (reference eval_parameter_homotopy)
+template <typename R, int W>
+__device__ __forceinline__ void coef_eval_p2c(const double* __restrict__ hx, const double* __restrict__ ht, int M,
+                                              int K, R t, cx<R>* c, cx<R>* cp, int l) {
+  for (int k = l; k <= M; k += W) {
+    const double* a = hx + 2 * (size_t)k * (K + 1);
+    cx<R> v = mk((R)__ldg(a + 2 * K), (R)__ldg(a + 2 * K + 1));
+    for (int j = K - 1; j >= 0; --j) v = mk(f_fma(v.re, t, (R)__ldg(a + 2 * j)), f_fma(v.im, t, (R)__ldg(a + 2 * j + 1)));
+    c[k] = v;
+    if (K >= 1) {
+      const double* b = ht + 2 * (size_t)k * K;
+      cx<R> u = mk((R)__ldg(b + 2 * (K - 1)), (R)__ldg(b + 2 * (K - 1) + 1));
+      for (int j = K - 2; j >= 0; --j) u = mk(f_fma(u.re, t, (R)__ldg(b + 2 * j)), f_fma(u.im, t, (R)__ldg(b + 2 * j + 1)));
+      cp[k] = u;
+    } else {
+      cp[k] = mk(R(0), R(0));
+    }
+  }
+}
+
+// p(t) = p1 t + p0 (1-t) and the parameter differences (reference compute_param_homotopy)
+template <typename R, int W>
+__device__ __forceinline__ void coef_eval_ph(const double* __restrict__ ps, const double* __restrict__ pt,
+                                             const double* __restrict__ pd, int P, R t, cx<R>* ph, cx<R>* dp,
+                                             int l) {
+  const R u = f_sub(R(1), t);
+  for (int k = l; k < P; k += W) {
+    const R gr = (R)__ldg(pt + 2 * k), gi = (R)__ldg(pt + 2 * k + 1);
+    const R sr = (R)__ldg(ps + 2 * k), si = (R)__ldg(ps + 2 * k + 1);
+    ph[k] = mk(f_fma(gr, t, f_mul(sr, u)), f_fma(gi, t, f_mul(si, u)));
+    dp[k] = mk((R)__ldg(pd + 2 * k), (R)__ldg(pd + 2 * k + 1));
+  }
+  if (l == 0) {
+    ph[P] = mk(R(1), R(0));
+    dp[P] = mk((R)__ldg(pd + 2 * P), (R)__ldg(pd + 2 * P + 1));
+  }
+}
+
+// Row r of H_x into A, and b = H (which = 0) or -H_t (which = 1).
+template <typename R, int N, int KIND>
+__device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, const cx<R>* cb, const cx<R>* xs, int r,
+                                         bool live, cx<R> (&A)[N], cx<R>& b, int which) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    cx<R> acc = mk(R(0), R(0));
+    if (live) {
+      const int j0 = tb.hx_off[r * N + i], j1 = tb.hx_off[r * N + i + 1];
+      for (int j = j0; j < j1; ++j) {
+        const uint64_t w = tb.hx_terms[j];
+        cx<R> p;
+        if (KIND == KIND_P2C) {
+          p = c_scale((R)term_scale(w), ca[term_coef(w)]);
+        } else {
+          p = c_scale((R)term_scale(w), ca[term_pa(w)]);
+          p = c_mul(p, ca[term_pb(w)]);
+        }
+        acc = acc_term(acc, p, w, xs);
+      }
+    }
+    A[i] = acc;
+  }
+  cx<R> h = mk(R(0), R(0));
+  if (live) {
+    const int j0 = tb.ht_off[r], j1 = tb.ht_off[r + 1];
+    for (int j = j0; j < j1; ++j) {
+      const uint64_t w = tb.ht_terms[j];
+      cx<R> p;
+      if (KIND == KIND_P2C) {
+        p = c_scale((R)term_scale(w), which ? cb[term_coef(w)] : ca[term_coef(w)]);
+      } else if (which) {
+        const int a = term_pa(w), bb = term_pb(w);
+        const cx<R> u = c_fma(cb[bb], ca[a], c_mul(cb[a], ca[bb]));
+        p = c_scale((R)term_scale(w), u);
+      } else {
+        p = c_scale((R)term_scale(w), ca[term_pa(w)]);
+        p = c_mul(p, ca[term_pb(w)]);
+      }
+      h = acc_term(h, p, w, xs);
+    }
+  }
+  b = which ? mk(-h.re, -h.im) : h;
+}
+
+// Partial-pivot LU + back substitution, one row per lane, rows in registers.
+// Pivot: max |Re|+|Im| over unpivoted rows, lowest position on ties; NaN at the
+// current position is kept, NaN elsewhere is never chosen (reference
+// dev-cgesv-batched-small.cuh:54-65).  Solution lands in sol[0..N).
+// sx holds N+1 entries (pivot row + its right-hand side).
+template <typename R, int N, int W>
+__device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
+  const bool live = l < N;
+  int pos = l;
+  cx<R> myrcp = mk(R(0), R(0));
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const R v = fabs(A[i].re) + fabs(A[i].im);
+    R key;
+    if (!live || pos < i) key = R(-2);
+    else if (v != v) key = (pos == i) ? (R)CUDART_INF : R(-1);
+    else key = v;
+    R bk = key;
+    int bp = pos;
+#pragma unroll
+    for (int off = W / 2; off > 0; off >>= 1) {
+      const R ok = shfl_xor(bk, off, W);
+      const int op = __shfl_xor_sync(kFull, bp, off, W);
+      if (ok > bk || (ok == bk && op < bp)) {
+        bk = ok;
+        bp = op;
+      }
+    }
+    const bool zero = (bk == R(0));
+    const bool is_piv = live && (pos == bp);
+    if (live) {
+      if (pos == bp) pos = i;
+      else if (pos == i) pos = bp;
+    }
+    if (is_piv) {
+#pragma unroll
+      for (int j = i; j < N; ++j) sx[j] = zero ? mk(R(0), R(0)) : A[j];
+      sx[N] = b;
+    }
+    __syncwarp(kFull);
+    const cx<R> rc = c_rcp(sx[i]);
+    if (is_piv) myrcp = rc;
+    const cx<R> reg = zero ? mk(R(1), R(0)) : rc;
+    if (live && pos > i) {
+      A[i] = c_mul(A[i], reg);
+#pragma unroll
+      for (int j = i + 1; j < N; ++j) A[j] = c_fnma(A[i], sx[j], A[j]);
+      b = c_fnma(A[i], sx[N], b);
+    }
+    __syncwarp(kFull);
+  }
+#pragma unroll
+  for (int i = N - 1; i >= 0; --i) {
+    if (live && pos == i) sol[i] = c_mul(b, myrcp);
+    __syncwarp(kFull);
+    const cx<R> xi = sol[i];
+    if (live && pos < i) b = c_fnma(A[i], xi, b);
+  }
+  __syncwarp(kFull);
+}
+
+// xor-butterfly sum over the first NP lanes of the sub-warp (order = oracle tree_sum)
+template <typename R, int N, int W>
+__device__ __forceinline__ R tree_sum(R v) {
+  constexpr int NP = (N <= 1) ? 1 : (N <= 2) ? 2 : (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
+  static_assert(NP <= W, "sub-warp narrower than the reduction tree");
+#pragma unroll
+  for (int off = NP / 2; off > 0; off >>= 1) v = f_add(v, shfl_xor(v, off, W));
+  return v;
+}
+
+// per-sub-warp shared-memory views
+struct SubMem {
+  unsigned char* coefA;  // c_k(t)   or p(t)     [Mc]
+  unsigned char* coefB;  // c'_k(t)  or p1 - p0  [Mc]
+  unsigned char* xs;     // track in stage precision [N+1]
+  unsigned char* sx;     // pivot row + rhs [N+1]
+  unsigned char* sol;    // solution [N]
+};
+
+template <typename R>
+__device__ __forceinline__ cx<R>* view(unsigned char* p) {
+  return reinterpret_cast<cx<R>*>(p);
+}
+
+// one evaluation + solve in precision R; returns this lane's solution component
+template <typename R, int N, int W, int KIND>
+__device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, int l, int which) {
+  cx<R> A[N];
+  cx<R> b;
+  eval_row<R, N, KIND>(tb, view<R>(sm.coefA), view<R>(sm.coefB), view<R>(sm.xs), l, l < N, A, b, which);
+  lu_solve<R, N, W>(A, b, l, view<R>(sm.sx), view<R>(sm.sol));
+  const cx<R> k = (l < N) ? view<R>(sm.sol)[l] : mk(R(0), R(0));
+  return k;
+}
+
+template <typename R, typename RS, int N>
+__device__ __forceinline__ void write_track(const SubMem& sm, int l, cx<RS> x) {
+  cx<R>* xs = view<R>(sm.xs);
+  if (l < N) xs[l] = c_cast<R>(x);
+  if (l == 0) xs[N] = mk(R(1), R(0));
+}
+
+template <typename R, int W, int KIND>
+__device__ __forceinline__ void coef_eval(const TrackParams& p, const SubMem& sm, long long hyp, R t, int l) {
+  if (KIND == KIND_P2C) {
+    coef_eval_p2c<R, W>(p.coef_hx + 2 * hyp * p.stride_hx, p.coef_ht + 2 * hyp * p.stride_ht, p.M, p.K, t,
+                        view<R>(sm.coefA), view<R>(sm.coefB), l);
+  } else {
+    coef_eval_ph<R, W>(p.p_start, p.p_tgt + 2 * hyp * p.stride_p, p.p_diff + 2 * hyp * p.stride_p, p.P, t,
+                       view<R>(sm.coefA), view<R>(sm.coefB), l);
+  }
+}
+
+// byte sizes of the shared-memory layout
+__host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+__host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
+  return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(N * N + 1 + N + 1));
+}
+__host__ __device__ inline size_t sub_bytes(int N, int Mc) {
+  return align16(16 * (size_t)(2 * Mc + (N + 1) + (N + 1) + N));
+}
+
+__device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64_t* g_hx, const uint16_t* g_hxo,
+                                               const uint64_t* g_ht, const uint16_t* g_hto, int N, int n_hx,
+                                               int n_ht) {
+  uint64_t* s_hx = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* s_ht = s_hx + n_hx;
+  uint16_t* s_hxo = reinterpret_cast<uint16_t*>(s_ht + n_ht);
+  uint16_t* s_hto = s_hxo + N * N + 1;
+  for (int i = threadIdx.x; i < n_hx; i += blockDim.x) s_hx[i] = __ldg(g_hx + i);
+  for (int i = threadIdx.x; i < n_ht; i += blockDim.x) s_ht[i] = __ldg(g_ht + i);
+  for (int i = threadIdx.x; i < N * N + 1; i += blockDim.x) s_hxo[i] = __ldg(g_hxo + i);
+  for (int i = threadIdx.x; i < N + 1; i += blockDim.x) s_hto[i] = __ldg(g_hto + i);
+  __syncthreads();
+  Tables t;
+  t.hx_terms = s_hx;
+  t.hx_off = s_hxo;
+  t.ht_terms = s_ht;
+  t.ht_off = s_hto;
+  return t;
+}
+
+// -------------------------------------------------------------------------------------------------
+// the tracker kernel
+//   RS  state precision (track, t, dt)      RP  predictor (RK) precision
+//   RCL corrector precision for t < t_switch RCH corrector precision for t >= t_switch
+// -------------------------------------------------------------------------------------------------
+template <typename RS, typename RP, typename RCL, typename RCH, int N, int W, int KIND>
+__global__ void __launch_bounds__(128) track_kernel(const TrackParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const Tables tb = stage_tables(smem, p.hx_terms, p.hx_off, p.ht_terms, p.ht_off, N, p.n_hx_terms, p.n_ht_terms);
+
+  const int lane = threadIdx.x & 31;
+  const int l = lane % W;
+  const int g = threadIdx.x / W;
+  const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
+  unsigned char* base = smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc);
+  SubMem sm;
+  sm.coefA = base;
+  sm.coefB = base + 16 * (size_t)Mc;
+  sm.xs = base + 32 * (size_t)Mc;
+  sm.sx = sm.xs + 16 * (N + 1);
+  sm.sol = sm.sx + 16 * (N + 1);
+
+  const int subs_per_cta = blockDim.x / W;
+  const long long n_sw = (long long)gridDim.x * subs_per_cta;
+  const int leader = lane - l;
+
+  // per-path state (replicated across the sub-warp's lanes)
+  long long item = (long long)blockIdx.x * subs_per_cta + g;
+  bool alive = item < p.n_items;
+  long long hyp = 0;
+  cx<RS> x = mk(RS(0), RS(0)), x0 = x, sols = x;
+  RS t0 = 0, dt = 0, t_step = 0;
+  bool end_zone = false, success = false, inf = false;
+  int nsucc = 0, step = 0, ncorr = 0;
+
+  const RS dt_init = (KIND == KIND_PH) ? RS(0.01) : RS(0.05);
+
+  auto init_path = [&](long long it) {
+    hyp = it / p.paths_per_hyp;
+    const long long pidx = it % p.paths_per_hyp;
+    const RS* st = reinterpret_cast<const RS*>(p.start_sols) + 2 * pidx * p.ld_start;
+    const RS* tr = p.track_in ? reinterpret_cast<const RS*>(p.track_in) + 2 * it * p.ld_track : st;
+    if (l < N) {
+      sols = mk(st[2 * l], st[2 * l + 1]);
+      x = mk(tr[2 * l], tr[2 * l + 1]);
+    } else {
+      sols = x = mk(RS(0), RS(0));
+    }
+    x0 = x;
+    t0 = 0;
+    dt = dt_init;
+    t_step = 0;
+    end_zone = false;
+    success = false;
+    inf = false;
+    nsucc = 0;
+    step = 0;
+    ncorr = 0;
+  };
+  if (alive) init_path(item);
+
+  while (__any_sync(kFull, alive)) {
+    // ---------------- step prologue: end-zone clamp (kernel_HC_Solver_P3P.cu:121-134)
+    RS half = 0;
+    if (alive) {
+      if (!end_zone && fabs(f_sub(RS(1), t0)) <= RS(0.0500001)) end_zone = true;
+      if (end_zone) {
+        const RS rem = fabs(f_sub(RS(1), t0));
+        if (dt > rem) dt = rem;
+      } else {
+        const RS edge = (KIND == KIND_PH) ? fabs(f_sub(RS(0.95), t0)) : fabs(f_sub(f_sub(RS(1), RS(0.05)), t0));
+        if (dt > edge) dt = edge;
+      }
+      t_step = t0;
+      half = f_mul(RS(0.5), dt);
+    }
+
+    // ---------------- loopy RK4 predictor (kernel_HC_Solver_P3P.cu:139-183)
+    cx<RS> k = mk(RS(0), RS(0));
+#pragma unroll 1
+    for (int rk = 0; rk < 4; ++rk) {
+      if (alive) coef_eval<RP, W, KIND>(p, sm, hyp, (RP)t0, l);
+      write_track<RP, RS, N>(sm, l, x);
+      __syncwarp(kFull);
+      k = c_cast<RS>(eval_solve<RP, N, W, KIND>(tb, sm, l, 1));
+      if (alive && rk < 3) {
+        const RS a = f_mul(dt, rk == 0 ? RS(1.0 / 6.0) : RS(2.0 / 6.0));
+        const RS d = f_mul(dt, rk == 2 ? RS(1.0) : RS(0.5));
+        sols = mk(f_fma(k.re, a, sols.re), f_fma(k.im, a, sols.im));
+        x = mk(f_fma(k.re, d, x0.re), f_fma(k.im, d, x0.im));
+        if (rk != 1) t0 = f_add(t0, half);
+      }
+    }
+    if (alive) {
+      const RS a = f_mul(dt, RS(1.0 / 6.0));
+      sols = mk(f_fma(k.re, a, sols.re), f_fma(k.im, a, sols.im));
+      x = sols;
+    }
+
+    // ---------------- Newton corrector (kernel_HC_Solver_P3P.cu:191-223)
+    const bool hi = !std::is_same<RCL, RCH>::value && alive && ((double)t0 >= p.t_switch);
+    if (!std::is_same<RCH, RP>::value) {
+      if (__any_sync(kFull, hi)) {
+        if (hi) coef_eval<RCH, W, KIND>(p, sm, hyp, (RCH)t0, l);
+        __syncwarp(kFull);
+      }
+    }
+    if (!std::is_same<RCL, RP>::value) {
+      if (__any_sync(kFull, alive && !hi)) {
+        if (alive && !hi) coef_eval<RCL, W, KIND>(p, sm, hyp, (RCL)t0, l);
+        __syncwarp(kFull);
+      }
+    }
+    bool running = alive;
+    success = false;
+    inf = false;
+#pragma unroll 1
+    for (int it = 0; it < p.max_corr; ++it) {
+      if (!__any_sync(kFull, running)) break;
+      // the low- and high-precision sub-warps of this warp (at most two passes)
+#pragma unroll
+      for (int pass = 0; pass < 2; ++pass) {
+        const bool mine = running && (pass == 0 ? !hi : hi);
+        if (pass == 1 && std::is_same<RCL, RCH>::value) break;
+        if (!__any_sync(kFull, mine)) continue;
+        cx<RS> dlt;
+        if (pass == 0) {
+          write_track<RCL, RS, N>(sm, l, x);
+          __syncwarp(kFull);
+          dlt = c_cast<RS>(eval_solve<RCL, N, W, KIND>(tb, sm, l, 0));
+        } else {
+          write_track<RCH, RS, N>(sm, l, x);
+          __syncwarp(kFull);
+          dlt = c_cast<RS>(eval_solve<RCH, N, W, KIND>(tb, sm, l, 0));
+        }
+        if (mine) x = c_sub(x, dlt);
+        const RS ns = tree_sum<RS, N, W>((mine && l < N) ? c_abs2(dlt) : RS(0));
+        const RS nc = tree_sum<RS, N, W>((mine && l < N) ? c_abs2(x) : RS(0));
+        const RS ns0 = __shfl_sync(kFull, ns, leader);
+        const RS nc0 = __shfl_sync(kFull, nc, leader);
+        if (mine) {
+          ++ncorr;
+          success = ((double)ns0 < 1e-6 * (double)nc0);
+          inf = ((double)nc0 > 1e14);
+          if (inf || success) running = false;
+        }
+      }
+    }
+
+    // ---------------- step control (kernel_HC_Solver_P3P.cu:225-249)
+    bool done = false;
+    if (alive) {
+      if (inf) {
+        done = true;
+      } else if (!success) {
+        dt = f_mul(dt, RS(0.5));
+        x = x0;
+        sols = x0;
+        nsucc = 0;
+        t0 = t_step;
+      } else {
+        ++nsucc;
+        x0 = x;
+        sols = x;
+        if (nsucc >= p.incr) {
+          nsucc = 0;
+          dt = f_mul(dt, RS(2));
+        }
+      }
+      ++step;
+      if (!done) done = !(t0 < RS(1) && f_sub(RS(1), t0) > RS(1e-7)) || step > p.max_steps;
+    }
+
+    // ---------------- finished paths: write out and take the next path
+    if (alive && done) {
+      RS* ep = reinterpret_cast<RS*>(p.endpoints) + 2 * item * p.ld_out;
+      if (l < N) {
+        ep[2 * l] = x.re;
+        ep[2 * l + 1] = x.im;
+      }
+      if (l == 0) {
+        const bool conv = (t0 >= RS(1) || f_sub(RS(1), t0) <= RS(1e-7));
+        if (p.conv) p.conv[item] = conv ? 1 : 0;
+        if (p.infy) p.infy[item] = inf ? 1 : 0;
+        if (p.status) p.status[item] = conv ? ST_CONVERGED : (inf ? ST_DIVERGED : ST_STEP_CAP);
+        if (p.steps) p.steps[item] = step;
+        if (p.corr) p.corr[item] = ncorr;
+        if (p.t_end) p.t_end[item] = (double)t0;
+        if (p.dt_end) p.dt_end[item] = (double)dt;
+      }
+    }
+    const bool need = alive && done;
+    long long nxt = 0;
+    if (need && l == 0) nxt = n_sw + (long long)atomicAdd(p.counter, 1);
+    nxt = __shfl_sync(kFull, nxt, leader);
+    if (need) {
+      item = nxt;
+      alive = item < p.n_items;
+      if (alive) init_path(item);
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------------------
+// Newton polish at t = 1 and the residual |H(x,1)| (double); one sub-warp per item
+// -------------------------------------------------------------------------------------------------
+template <int N, int W, int KIND>
+__global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const Tables tb = stage_tables(smem, p.hx_terms, p.hx_off, p.ht_terms, p.ht_off, N, p.n_hx_terms, p.n_ht_terms);
+  const int lane = threadIdx.x & 31;
+  const int l = lane % W;
+  const int g = threadIdx.x / W;
+  const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
+  unsigned char* base = smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc);
+  SubMem sm;
+  sm.coefA = base;
+  sm.coefB = base + 16 * (size_t)Mc;
+  sm.xs = base + 32 * (size_t)Mc;
+  sm.sx = sm.xs + 16 * (N + 1);
+  sm.sol = sm.sx + 16 * (N + 1);
+  const int subs_per_cta = blockDim.x / W;
+  const int leader = lane - l;
+  for (long long item0 = (long long)blockIdx.x * subs_per_cta; item0 < p.n_items;
+       item0 += (long long)gridDim.x * subs_per_cta) {
+    const long long item = item0 + g;
+    const bool valid = item < p.n_items;
+    const bool conv = valid && p.conv[item];
+    const long long hyp = valid ? item / p.paths_per_hyp : 0;
+    double* ep = p.endpoints + 2 * (valid ? item : 0) * p.ld;
+    cx<double> x = (valid && l < N) ? mk(ep[2 * l], ep[2 * l + 1]) : mk(0.0, 0.0);
+    if (conv) {
+      if (KIND == KIND_P2C) {
+        coef_eval_p2c<double, W>(p.coef_hx + 2 * hyp * p.stride_hx, p.coef_ht + 2 * hyp * p.stride_ht, p.M, p.K,
+                                 1.0, view<double>(sm.coefA), view<double>(sm.coefB), l);
+      } else {
+        coef_eval_ph<double, W>(p.p_start, p.p_tgt + 2 * hyp * p.stride_p, p.p_diff + 2 * hyp * p.stride_p, p.P,
+                                1.0, view<double>(sm.coefA), view<double>(sm.coefB), l);
+      }
+    }
+    __syncwarp(kFull);
+    for (int it = 0; it < p.iters; ++it) {
+      write_track<double, double, N>(sm, l, x);
+      __syncwarp(kFull);
+      const cx<double> d = eval_solve<double, N, W, KIND>(tb, sm, l, 0);
+      if (conv) x = c_sub(x, d);
+    }
+    // residual |H(x,1)|
+    write_track<double, double, N>(sm, l, x);
+    __syncwarp(kFull);
+    cx<double> A[N];
+    cx<double> h;
+    eval_row<double, N, KIND>(tb, view<double>(sm.coefA), view<double>(sm.coefB), view<double>(sm.xs), l, l < N, A,
+                              h, 0);
+    const double s = tree_sum<double, N, W>(l < N ? c_abs2(h) : 0.0);
+    const double s0 = __shfl_sync(kFull, s, leader);
+    if (valid) {
+      if (conv && l < N) {
+        ep[2 * l] = x.re;
+        ep[2 * l + 1] = x.im;
+      }
+      if (l == 0 && p.resid) p.resid[item] = conv ? sqrt(s0) : -1.0;
+    }
+    __syncwarp(kFull);
+  }
+}
+
+}  // namespace dev
+}  // namespace ghc

@@ -1,0 +1,80 @@
+// tracker_launch.cuh -- launch templates shared by the per-precision translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ghc_internal.h"
+#include "tracker.cuh"
+
+namespace ghc {
+namespace launch_detail {
+
+constexpr int kBlock = 128;
+
+template <typename RS, typename RP, typename RCL, typename RCH, int N, int KIND>
+int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
+  constexpr int W = (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
+  auto kern = dev::track_kernel<RS, RP, RCL, RCH, N, W, KIND>;
+  const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
+  const int subs = kBlock / W;
+  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return -20;
+  int occ = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlock, smem);
+  if (e != cudaSuccess || occ < 1) return -21;
+  // persistent grid: fill the GPU once, but never launch more sub-warps than items
+  long long grid = (long long)occ * n_sm;
+  const long long need = (p.n_items + subs - 1) / subs;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  e = cudaMemsetAsync(p.counter, 0, sizeof(int), s);
+  if (e != cudaSuccess) return -22;
+  kern<<<(unsigned)grid, kBlock, smem, s>>>(p);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : -23;
+}
+
+template <int N, int KIND>
+int launch_polish_t(const PolishParams& p, cudaStream_t s) {
+  constexpr int W = (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
+  auto kern = dev::polish_kernel<N, W, KIND>;
+  const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
+  const int subs = kBlock / W;
+  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc);
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -20;
+  long long grid = (p.n_items + subs - 1) / subs;
+  if (grid > 65535LL * 16) grid = 65535LL * 16;
+  if (grid < 1) grid = 1;
+  kern<<<(unsigned)grid, kBlock, smem, s>>>(p);
+  return cudaGetLastError() == cudaSuccess ? 0 : -23;
+}
+
+}  // namespace launch_detail
+
+
+#define GHC_P2C_SIZES(X) X(3) X(4) X(5) X(6) X(8) X(10) X(11) X(12) X(16) X(18)
+
+// dispatch of one precision mode over the compiled sizes
+template <typename RS, typename RP, typename RCL, typename RCH>
+int launch_mode(const TrackParams& p, cudaStream_t s, int n_sm) {
+  using namespace launch_detail;
+  if (p.kind == KIND_P2C) {
+    switch (p.N) {
+#define CASE(n) \
+  case n:       \
+    return launch_track_t<RS, RP, RCL, RCH, n, KIND_P2C>(p, s, n_sm);
+      GHC_P2C_SIZES(CASE)
+#undef CASE
+      default:
+        return -10;
+    }
+  }
+  if (p.kind == KIND_PH && p.N == 30) return launch_track_t<RS, RP, RCL, RCH, 30, KIND_PH>(p, s, n_sm);
+  return -10;
+}
+
+int launch_track_fp64(const TrackParams& p, cudaStream_t s, int n_sm);
+int launch_track_fp32(const TrackParams& p, cudaStream_t s, int n_sm);
+int launch_track_mixed(const TrackParams& p, cudaStream_t s, int n_sm);
+
+}  // namespace ghc

@@ -1,0 +1,66 @@
+/*
+ * hc_oracle.c -- CPU oracle of the homotopy path tracker.
+ *
+ * TEST INFRASTRUCTURE ONLY: a plain-C restatement of the reference tracker,
+ * used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
+ * the checker.  The product never links or calls it.
+ *
+ * The precision-generic body lives in hc_oracle_body.h and is instantiated
+ * for double (suffix _d) and float (suffix _f).  Build flags (oracle/build.py):
+ * -O2 -ffp-contract=off -fopenmp, so no multiply-add is fused except through
+ * the explicit fma()/fmaf() calls.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_NMAX 32
+#define ORC_MMAX 640
+
+enum { ORC_P2C = 0, ORC_PH = 1 };
+enum { ORC_CONVERGED = 0, ORC_DIVERGED = 1, ORC_STEP_CAP = 2 };
+
+/* Problem description: the YAML sizes plus the raw index tables in the
+ * reference layout (GPU-HC/magmaHC/GPU_HC_Solver.cpp:44-83). */
+typedef struct {
+  int32_t kind; /* ORC_P2C or ORC_PH */
+  int32_t N, P, M, K;
+  int32_t Tx, Px, Tt, Pt;
+  int32_t max_steps, max_corr, incr_steps;
+  int32_t polish_iters;
+  const int32_t* hx_idx;
+  const int32_t* ht_idx;
+} orc_problem;
+
+typedef struct {
+  uint8_t converged, infinity, status;
+  int32_t steps, corr;
+  double t_end, dt_end, resid;
+} orc_path_out;
+
+#define REAL double
+#define SUFFIX _d
+#define FMA fma
+#define FABS fabs
+#include "hc_oracle_body.h"
+#undef REAL
+#undef SUFFIX
+#undef FMA
+#undef FABS
+
+#define REAL float
+#define SUFFIX _f
+#define FMA fmaf
+#define FABS fabsf
+#include "hc_oracle_body.h"
+#undef REAL
+#undef SUFFIX
+#undef FMA
+#undef FABS
+
+int orc_abi_version(void) { return 1; }
+int orc_sizeof_problem(void) { return (int)sizeof(orc_problem); }

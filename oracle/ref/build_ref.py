@@ -1,0 +1,132 @@
+"""Compile the reference's P2C coefficient builders into oracle/_ref/.
+
+TEST INFRASTRUCTURE ONLY.  The reference's host-side P2C functions
+(GPU-HC/magmaHC/PHC_Coeffs/p2c-<problem>.h, namespace magmaHCWrapper) are
+plain C++ over MAGMA's complex type.  They are compiled here from their own
+sources, where they lie in the reference tree, against the stand-in header in
+oracle/ref/shim/ (a small complex struct), once in double and once in float.
+
+Output: oracle/_ref/libp2c_ref.so with, per problem <p>,
+    void ref_p2c_<p>_d(const double* tgt, const double* start, double* hx, double* ht)
+    void ref_p2c_<p>_f(const float*  tgt, const float*  start, float*  hx, float*  ht)
+(complex arrays interleaved re, im; tgt/start hold P+1 entries, hx
+(M+1)(K+1), ht (M+1)K).  The reference's tracker kernels themselves need
+MAGMA's internal device headers, which are not part of the reference tree,
+so they are not buildable here.
+"""
+import glob
+import os
+import re
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE = os.path.dirname(HERE)
+OUT = os.path.join(ORACLE, "_ref")
+LIB = os.path.join(OUT, "libp2c_ref.so")
+DEFAULT_ROOT = "/root/reference"
+
+WRAP_HEAD = """// generated by oracle/ref/build_ref.py -- wrappers around the reference P2C builders
+#include <cstddef>
+#include <stdio.h>
+#include <stdlib.h>
+#include <cstdio>
+#include <cstdlib>
+#include <iostream>
+#include <iomanip>
+#include <cstring>
+#include <chrono>
+#define REF_REAL %(real)s
+#define ref_cx ref_cx_%(tag)s
+#include "magma_v2.h"
+namespace ref_%(tag)s {
+%(includes)s
+}
+namespace {
+template <int Dummy>
+struct Buf {
+  static void load(const REF_REAL* s, ref_cx* d, int n) { for (int i = 0; i < n; ++i) d[i] = ref_cx(s[2*i], s[2*i+1]); }
+  static void store(const ref_cx* s, REF_REAL* d, int n) { for (int i = 0; i < n; ++i) { d[2*i] = s[i].x; d[2*i+1] = s[i].y; } }
+};
+}
+"""
+
+WRAP_FN = """extern "C" void ref_p2c_%(name)s_%(tag)s(const REF_REAL* tgt, const REF_REAL* st, REF_REAL* hx, REF_REAL* ht) {
+  static const int NP = 4096;
+  ref_cx T[NP], S[NP], HX[NP], HT[NP];
+  Buf<0>::load(tgt, T, %(np)d); Buf<0>::load(st, S, %(np)d);
+  ref_%(tag)s::magmaHCWrapper::p2c_%(name)s(T, S, HX, HT);
+  Buf<0>::store(HX, hx, %(nhx)d); Buf<0>::store(HT, ht, %(nht)d);
+}
+"""
+
+
+def _yaml(path):
+    d = {}
+    for line in open(path):
+        line = line.split("#", 1)[0]
+        m = re.match(r"\s*(\w+)\s*:\s*(\S+)", line)
+        if m:
+            d[m.group(1)] = m.group(2)
+    return d
+
+
+PKG_PROBLEMS = os.path.join(os.path.dirname(ORACLE), "homotopy-continuation-tracker-on-gpu_b200", "problems")
+
+
+def problems_with_p2c(root):
+    """P2C problems of the reference that this package imports."""
+    wanted = set(os.listdir(PKG_PROBLEMS)) if os.path.isdir(PKG_PROBLEMS) else None
+    out = []
+    for hdr in sorted(glob.glob(os.path.join(root, "GPU-HC/magmaHC/PHC_Coeffs/p2c-*.h"))):
+        name = os.path.basename(hdr)[4:-2]
+        if wanted is not None and name not in wanted:
+            continue
+        ydir = os.path.join(root, "GPU-HC/problems", name)
+        if not os.path.isdir(ydir):
+            continue  # the numeric-only 6-lines builder has no same-named problem folder
+        y = _yaml(os.path.join(ydir, "gpuhc_settings.yaml"))
+        if y.get("GPUHC_Type") != "P2C":
+            continue
+        P, M, K = int(y["Num_Of_Params"]), int(y["Num_Of_Coeffs_From_Params"]), int(y["Max_Order_Of_T"])
+        out.append((name, hdr, P, M, K))
+    return out
+
+
+def build(root=DEFAULT_ROOT, force=False, verbose=False):
+    if not os.path.isdir(os.path.join(root, "GPU-HC")):
+        return None
+    os.makedirs(OUT, exist_ok=True)
+    probs = problems_with_p2c(root)
+    if (not force) and os.path.exists(LIB):
+        newest = max([os.path.getmtime(__file__)] + [os.path.getmtime(p[1]) for p in probs])
+        if os.path.getmtime(LIB) >= newest:
+            return LIB
+    objs = []
+    for real, tag in (("double", "d"), ("float", "f")):
+        includes = "\n".join('#include "%s"' % p[1] for p in probs)
+        src = WRAP_HEAD % dict(real=real, tag=tag, includes=includes)
+        for name, _, P, M, K in probs:
+            src += WRAP_FN % dict(name=name, tag=tag, np=P + 1, nhx=(M + 1) * (K + 1), nht=(M + 1) * K)
+        cpp = os.path.join(OUT, "p2c_ref_%s.cpp" % tag)
+        with open(cpp, "w") as f:
+            f.write(src)
+        obj = cpp[:-4] + ".o"
+        cmd = ["g++", "-O0", "-std=c++14", "-fPIC", "-w", "-I", os.path.join(HERE, "shim"),
+               "-c", cpp, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+        objs.append(obj)
+    tmp = LIB + ".tmp%d" % os.getpid()
+    subprocess.check_call(["g++", "-shared", "-o", tmp] + objs)
+    os.replace(tmp, LIB)
+    with open(os.path.join(OUT, "problems.txt"), "w") as f:
+        for name, _, P, M, K in probs:
+            f.write("%s %d %d %d\n" % (name, P, M, K))
+    return LIB
+
+
+if __name__ == "__main__":
+    root = sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith("-") else DEFAULT_ROOT
+    print(build(root, force="--force" in sys.argv, verbose=True))

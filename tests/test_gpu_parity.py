@@ -1,0 +1,224 @@
+"""GPU tracker vs the CPU oracle on identical inputs (needs a B200).
+
+FP64 and FP32 modes follow the oracle's operation order, so endpoints, flags
+and step/iteration counters must be identical (compared as values).  Mixed
+precision is checked by recall of the FP64 real endpoints after FP64 polish.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import ghc
+import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+SUPPORTED = ["P3P", "5pt_rel_pos_alg_form_quat", "generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY",
+             "3view_triangulation", "6pt_RS_abs_pos", "dual_reciever_TDOA_5pt", "distorted_2view_triangulation",
+             "P3P_10x10", "trifocal_2op1p_30x30"]
+NCPU = os.cpu_count() or 1
+
+
+def cx_t(a, dtype=torch.float64):
+    a = np.asarray(a, dtype=np.complex128)
+    return torch.from_numpy(np.ascontiguousarray(np.stack([a.real, a.imag], -1))).to(dtype).cuda()
+
+
+def to_cx(t):
+    a = t.double().cpu().numpy()
+    return a[..., 0] + 1j * a[..., 1]
+
+
+def inputs(name, n_hyp=1, seed=0):
+    """problem handles + per-hypothesis targets (hypothesis 0 = shipped target)."""
+    pb, ob = ghc.Problem(name), O.Problem(name)
+    rng = np.random.default_rng(seed)
+    tg = [ob.target_params]
+    for _ in range(n_hyp - 1):
+        # small seeded perturbations of the shipped target keep the problems well posed
+        d = 0.05 * (rng.normal(size=ob.P) + 1j * rng.normal(size=ob.P))
+        tg.append(np.append(ob.target_params[:-1] + d, 1.0))
+    return pb, ob, np.array(tg)
+
+
+def run_gpu(pb, ob, targets, precision, polish=0, **kw):
+    n_hyp = len(targets)
+    rt = torch.float32 if precision == ghc.PREC_FP32 else torch.float64
+    ws = ghc.Workspace(pb, n_hyp, precision)
+    ss = cx_t(ob.start_sols, rt)
+    if pb.kind == ghc.KIND_P2C:
+        hx = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[0] for t in targets])
+        ht = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[1] for t in targets])
+        ghc.track(pb, ws, ss, d_coef_hx=cx_t(hx), d_coef_ht=cx_t(ht), polish_iters=polish, **kw)
+        oargs = dict(hx=hx, ht=ht)
+    else:
+        ps = cx_t(ob.start_params)
+        pt = cx_t(targets)
+        pd = cx_t(targets - ob.start_params[None, :])
+        ghc.track(pb, ws, ss, d_p_start=ps, d_p_target=pt, d_p_diff=pd, polish_iters=polish, **kw)
+        oargs = dict(p_start=ob.start_params, p_target=targets)
+    torch.cuda.synchronize()
+    return ws, oargs
+
+
+def compare(ws, r, exact=True):
+    ep = to_cx(ws.endpoints)
+    assert np.array_equal(ws.conv.cpu().numpy(), r["conv"])
+    assert np.array_equal(ws.inf.cpu().numpy(), r["inf"])
+    assert np.array_equal(ws.status.cpu().numpy(), r["status"])
+    assert np.array_equal(ws.steps.cpu().numpy(), r["steps"])
+    assert np.array_equal(ws.corr.cpu().numpy(), r["corr"])
+    assert np.array_equal(ws.t_end.cpu().numpy(), r["t_end"])
+    fin = np.isfinite(r["endpoints"])
+    assert np.array_equal(np.isfinite(ep), fin)
+    assert np.array_equal(ep[fin], r["endpoints"][fin])
+
+
+@pytest.mark.parametrize("name", SUPPORTED)
+def test_fp64_bit_exact_vs_oracle(name):
+    pb, ob, tg = inputs(name)
+    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_FP64, polish=2)
+    r = O.track(ob, ob.start_sols, polish_iters=2, nthreads=NCPU, **oargs)
+    compare(ws, r)
+    res = ws.resid.cpu().numpy()
+    conv = r["conv"] == 1
+    assert np.array_equal(res[conv], r["resid"][conv])
+    assert ghc.count_results(to_cx(ws.endpoints), ws.conv.cpu().numpy(), ws.inf.cpu().numpy()) == \
+        O.count_results(r["endpoints"], r["conv"], r["inf"])
+
+
+@pytest.mark.parametrize("name", ["P3P", "generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY",
+                                  "trifocal_2op1p_30x30", "5pt_rel_pos_alg_form_quat"])
+def test_fp32_bit_exact_vs_oracle(name):
+    pb, ob, tg = inputs(name)
+    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_FP32)
+    oargs = {k: (v.astype(np.complex64) if isinstance(v, np.ndarray) else v) for k, v in oargs.items()}
+    r = O.track(ob, ob.start_sols.astype(np.complex64), precision="f", nthreads=NCPU, **oargs)
+    compare(ws, r)
+
+
+@pytest.mark.parametrize("name", ["P3P", "generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY"])
+def test_batched_hypotheses_equal_single_runs(name):
+    pb, ob, tg = inputs(name, n_hyp=3, seed=5)
+    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_FP64)
+    r = O.track(ob, ob.start_sols, nthreads=NCPU, **oargs)
+    compare(ws, r)
+    # hypothesis 2 alone gives the same results as inside the batch
+    ws1, _ = run_gpu(pb, ob, tg[2:3], ghc.PREC_FP64)
+    n = pb.paths
+    assert np.array_equal(to_cx(ws1.endpoints), to_cx(ws.endpoints)[2 * n:3 * n])
+    assert np.array_equal(ws1.steps.cpu().numpy(), ws.steps.cpu().numpy()[2 * n:3 * n])
+
+
+@pytest.mark.parametrize("name", ["generalized_3views_4pts", "5pt_rel_pos_alg_form_quat", "P3P"])
+def test_mixed_precision_recall(name):
+    """FP32 predictor / FP64 end-game: >= 99.5% of the FP64 run's real endpoints found within 1e-8."""
+    pb, ob, tg = inputs(name, n_hyp=2, seed=9)
+    w64, _ = run_gpu(pb, ob, tg, ghc.PREC_FP64, polish=3)
+    wmx, _ = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=3, t_switch=0.9)
+    e64, emx = to_cx(w64.endpoints), to_cx(wmx.endpoints)
+    c64, cmx = w64.conv.cpu().numpy() == 1, wmx.conv.cpu().numpy() == 1
+    r64 = w64.resid.cpu().numpy()
+    real64 = c64 & (np.abs(e64.imag).max(axis=1) <= 1e-8) & (r64 < 1e-10)
+    found = 0
+    n = pb.paths
+    for i in np.nonzero(real64)[0]:
+        h = i // n
+        cand = emx[h * n:(h + 1) * n][cmx[h * n:(h + 1) * n]]
+        err = np.abs(cand - e64[i]).max(axis=1) / max(1.0, np.abs(e64[i]).max())
+        found += bool(err.size and err.min() <= 1e-8)
+    assert real64.sum() > 0
+    assert found >= 0.995 * real64.sum(), (found, real64.sum())
+    rmx = wmx.resid.cpu().numpy()[cmx]
+    assert np.median(rmx) < 1e-10
+
+
+def test_step_cap_and_short_corrector():
+    pb, ob, tg = inputs("generalized_3views_4pts")
+    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_FP64, max_steps=5, max_corr=2)
+    r = O.track(ob, ob.start_sols, nthreads=NCPU, max_steps=5, max_corr=2, **oargs)
+    compare(ws, r)
+    assert (ws.status.cpu().numpy() == ghc.STATUS_STEP_CAP).any()
+
+
+def test_device_p2c_matches_host():
+    pb, ob, tg = inputs("generalized_3views_4pts", n_hyp=4, seed=3)
+    hx, ht = pb.p2c_device(cx_t(ob.start_params), cx_t(tg))
+    torch.cuda.synchronize()
+    for h in range(4):
+        rhx, rht = pb.p2c(ob.start_params, tg[h])
+        assert np.allclose(to_cx(hx[h]), rhx, rtol=1e-14, atol=1e-13 * np.abs(rhx).max())
+        assert np.allclose(to_cx(ht[h])[: len(rht)], rht, rtol=1e-14, atol=1e-13 * np.abs(rht).max())
+
+
+def test_empty_batch_is_a_noop():
+    pb, ob, tg = inputs("P3P")
+    ws = ghc.Workspace(pb, 0, ghc.PREC_FP64)
+    hx = torch.zeros((0, (pb.M + 1) * (pb.K + 1), 2), dtype=torch.float64, device="cuda")
+    ghc.track(pb, ws, cx_t(ob.start_sols), d_coef_hx=hx, d_coef_ht=hx)
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("name,prec", [("generalized_3views_4pts", ghc.PREC_FP64), ("P3P", ghc.PREC_FP32),
+                                       ("trifocal_2op1p_30x30", ghc.PREC_FP64)])
+def test_solve_host_end_to_end(name, prec):
+    pb, ob, tg = inputs(name)
+    out = ghc.solve_host(pb, prec)
+    ws, oargs = run_gpu(pb, ob, tg, prec)
+    assert np.array_equal(out["conv"], ws.conv.cpu().numpy())
+    assert np.array_equal(out["endpoints"], to_cx(ws.endpoints))
+
+
+@pytest.mark.parametrize("name,prec", [("P3P", "f"), ("uncalibrated_trifocal_rel_pos_CY", "f"),
+                                       ("generalized_3views_4pts", "d"), ("trifocal_2op1p_30x30", "f"),
+                                       ("trifocal_2op1p_30x30", "d")])
+def test_dropin_reference_abi(name, prec):
+    """kernel_HC_Solver_<p>-style call: pointer arrays, reference layout [N+1], bool flags, debug (t, dt)."""
+    import ctypes
+    pb, ob, tg = inputs(name)
+    rt = torch.float32 if prec == "f" else torch.float64
+    N, n = pb.N, pb.paths
+    sols = np.concatenate([ob.start_sols, np.ones((n, 1))], axis=1)
+    d_start = cx_t(sols, rt)
+    d_track = cx_t(sols, rt)
+    esz = 2 * (4 if prec == "f" else 8)
+    p_start = torch.tensor([d_start.data_ptr() + i * (N + 1) * esz for i in range(n)], dtype=torch.int64).cuda()
+    p_track = torch.tensor([d_track.data_ptr() + i * (N + 1) * esz for i in range(n)], dtype=torch.int64).cuda()
+    hxr, htr = ob.hx_idx, ob.ht_idx
+    d_hxi = torch.from_numpy(hxr).cuda()
+    d_hti = torch.from_numpy(htr).cuda()
+    conv = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    inf = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    dbg = torch.zeros((n, 2), dtype=rt, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    if pb.kind == ghc.KIND_P2C:
+        hx, ht = O.p2c_tables(ob.terms, ob.start_params, ob.target_params)
+        fn = ghc.ghc_kernel_HC_Solver_P2C if prec == "f" else ghc.ghc_kernel_HC_Solver_P2C_z
+        sec = fn(pb.h, st, pb.max_steps, pb.max_corr, pb.incr_steps, p_start.data_ptr(), p_track.data_ptr(),
+                 d_hxi.data_ptr(), d_hti.data_ptr(), cx_t(hx, rt).data_ptr(), cx_t(ht, rt).data_ptr(),
+                 conv.data_ptr(), inf.data_ptr(), dbg.data_ptr())
+        oargs = dict(hx=hx, ht=ht)
+    else:
+        fn = ghc.ghc_kernel_HC_Solver_PH if prec == "f" else ghc.ghc_kernel_HC_Solver_PH_z
+        ps, pt = ob.start_params, ob.target_params
+        keep = [cx_t(ps, rt), cx_t(pt, rt), cx_t(pt - ps, rt)]
+        sec = fn(pb.h, st, pb.max_steps, pb.max_corr, pb.incr_steps, p_start.data_ptr(), p_track.data_ptr(),
+                 keep[0].data_ptr(), keep[1].data_ptr(), keep[2].data_ptr(), d_hxi.data_ptr(), d_hti.data_ptr(),
+                 conv.data_ptr(), inf.data_ptr(), dbg.data_ptr())
+        oargs = dict(p_start=ps, p_target=pt[None, :])
+    assert sec >= 0, ghc.ghc_last_error()
+    if prec == "f":
+        oargs = {k: (v.astype(np.complex64) if isinstance(v, np.ndarray) else v) for k, v in oargs.items()}
+    r = O.track(ob, ob.start_sols.astype(np.complex64 if prec == "f" else np.complex128), precision=prec,
+                nthreads=NCPU, **oargs)
+    ep = to_cx(d_track)[:, :N]
+    assert np.array_equal(conv.cpu().numpy(), r["conv"])
+    assert np.array_equal(inf.cpu().numpy(), r["inf"])
+    fin = np.isfinite(r["endpoints"])
+    assert np.array_equal(ep[fin], r["endpoints"][fin])
+    d = to_cx(dbg)
+    c = r["conv"] == 1
+    assert np.all(d[c] == 1)
+    assert np.allclose(d[~c].real, r["t_end"][~c]) and np.allclose(d[~c].imag, r["dt_end"][~c])

@@ -80,20 +80,14 @@ template <typename R>
 __device__ __forceinline__ cx<R> c_fnma(cx<R> a, cx<R> b, cx<R> c) {
   return mk(f_fma(-a.re, b.re, f_fma(a.im, b.im, c.re)), f_fma(-a.re, b.im, f_fma(-a.im, b.re, c.im)));
 }
-// 1/b, Smith (1962) with one reciprocal of the scaled denominator
+// 1/b = conj(b) / |b|^2 with one correctly rounded reciprocal
+__device__ __forceinline__ double f_rcp(double a) { return __drcp_rn(a); }
+__device__ __forceinline__ float f_rcp(float a) { return __frcp_rn(a); }
 template <typename R>
 __device__ __forceinline__ cx<R> c_rcp(cx<R> b) {
-  if (fabs(b.re) >= fabs(b.im)) {
-    const R r = f_div(b.im, b.re);
-    const R d = f_fma(b.im, r, b.re);
-    const R inv = f_div(R(1), d);
-    return mk(inv, -f_mul(r, inv));
-  } else {
-    const R r = f_div(b.re, b.im);
-    const R d = f_fma(b.re, r, b.im);
-    const R inv = f_div(R(1), d);
-    return mk(f_mul(r, inv), -inv);
-  }
+  const R s = f_fma(b.re, b.re, f_mul(b.im, b.im));
+  const R inv = f_rcp(s);
+  return mk(f_mul(b.re, inv), -f_mul(b.im, inv));
 }
 template <typename R>
 __device__ __forceinline__ R c_abs2(cx<R> a) {

@@ -31,8 +31,8 @@
  *     reference reads them without the hypothesis offset);
  *   - padding terms (integer scale 0) are skipped and variable slot N (the
  *     constant 1) is not multiplied in;
- *   - complex division is Smith's algorithm (1962); the back substitution
- *     multiplies by the reciprocal of the pivot formed during elimination.
+ *   - the pivot reciprocal is conj(b)/|b|^2 (one reciprocal); the back
+ *     substitution multiplies by the reciprocal formed during elimination.
  */
 
 #define CAT2(a, b) a##b
@@ -58,19 +58,11 @@ static inline CX SFX(c_fma)(CX a, CX b, CX c) {
 static inline CX SFX(c_fnma)(CX a, CX b, CX c) {
   return SFX(c_make)(FMA(-a.re, b.re, FMA(a.im, b.im, c.re)), FMA(-a.re, b.im, FMA(-a.im, b.re, c.im)));
 }
-/* 1/b by Smith's algorithm (one reciprocal of the scaled denominator) */
+/* 1/b = conj(b) / |b|^2 with one correctly rounded reciprocal */
 static inline CX SFX(c_rcp)(CX b) {
-  if (FABS(b.re) >= FABS(b.im)) {
-    REAL r = b.im / b.re;
-    REAL d = FMA(b.im, r, b.re);
-    REAL inv = (REAL)1 / d;
-    return SFX(c_make)(inv, -(r * inv));
-  } else {
-    REAL r = b.re / b.im;
-    REAL d = FMA(b.re, r, b.im);
-    REAL inv = (REAL)1 / d;
-    return SFX(c_make)(r * inv, -inv);
-  }
+  const REAL s = FMA(b.re, b.re, b.im * b.im);
+  const REAL inv = (REAL)1 / s;
+  return SFX(c_make)(b.re * inv, -(b.im * inv));
 }
 /* |a|^2 */
 static inline REAL SFX(c_abs2)(CX a) { return FMA(a.re, a.re, a.im * a.im); }

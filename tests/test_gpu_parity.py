@@ -56,7 +56,11 @@ def run_gpu(pb, ob, targets, precision, polish=0, **kw):
     else:
         ps = cx_t(ob.start_params)
         pt = cx_t(targets)
-        pd = cx_t(targets - ob.start_params[None, :])
+        if precision == ghc.PREC_FP32:
+            # the FP32 oracle subtracts in float: hand the kernel the same rounded difference
+            pd = cx_t(targets.astype(np.complex64) - ob.start_params.astype(np.complex64)[None, :])
+        else:
+            pd = cx_t(targets - ob.start_params[None, :])
         ghc.track(pb, ws, ss, d_p_start=ps, d_p_target=pt, d_p_diff=pd, polish_iters=polish, **kw)
         oargs = dict(p_start=ob.start_params, p_target=targets)
     torch.cuda.synchronize()

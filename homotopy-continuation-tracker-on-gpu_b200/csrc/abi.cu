@@ -73,6 +73,10 @@ TrackParams base_params(const Problem& pb) {
   p.ht_terms = pb.dev.ht_terms;
   p.ht_off = pb.dev.ht_off;
   p.t_switch = 2.0;
+  // the reference's step control (kernel_HC_Solver_P3P.cu:214): no contraction test, no step cap
+  p.corr_tol2 = 1e-6;
+  p.first_tol2 = HUGE_VAL;
+  p.dt_max = HUGE_VAL;
   return p;
 }
 
@@ -373,7 +377,12 @@ int ghc_p2c_device(const ghc_problem* h, int64_t n_hyp, const double* d_start, c
 }
 
 int ghc_track(const ghc_problem* h, const ghc_track_args* a, void* stream) {
-  if (!h || !a || !a->d_start_sols || !a->d_endpoints || !a->d_counter || a->n_hyp < 0) {
+  if (!h || !a || a->n_hyp < 0) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  if (a->n_hyp == 0) return GHC_OK;
+  if (!a->d_start_sols || !a->d_endpoints || !a->d_counter) {
     set_error("null argument");
     return GHC_ERR_ARG;
   }
@@ -421,6 +430,9 @@ int ghc_track(const ghc_problem* h, const ghc_track_args* a, void* stream) {
   p.counter = a->d_counter;
   p.t_switch = a->t_switch;
   if (a->precision == GHC_PREC_FP64) p.t_switch = 2.0;
+  if (a->corr_tol2 > 0) p.corr_tol2 = a->corr_tol2;
+  if (a->first_tol2 > 0) p.first_tol2 = a->first_tol2;
+  if (a->dt_max > 0) p.dt_max = a->dt_max;
   rc = track_code(launch_track(p, a->precision, stream, sm_count()));
   if (rc) return rc;
   const bool fp64_state = a->precision == GHC_PREC_FP64 || a->precision == GHC_PREC_MIXED;

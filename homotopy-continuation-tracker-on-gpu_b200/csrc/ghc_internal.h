@@ -79,6 +79,10 @@ struct TrackParams {
   int* counter;            // one int, zero before launch
   // mixed precision: corrector in the high precision once t >= t_switch
   double t_switch;
+  // step control (reference: corr_tol2 = 1e-6, first_tol2 = dt_max = +inf)
+  double corr_tol2;   // corrector success: |dx|^2 < corr_tol2 |x|^2
+  double first_tol2;  // reject when the first Newton update has |dx|^2 > first_tol2 |x|^2
+  double dt_max;      // step-size cap
 };
 
 struct PolishParams {

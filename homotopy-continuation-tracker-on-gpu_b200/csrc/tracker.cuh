@@ -320,8 +320,8 @@ __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t
 __host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
   return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(N * N + 1 + N + 1));
 }
-__host__ __device__ inline size_t sub_bytes(int N, int Mc) {
-  return align16(16 * (size_t)(2 * Mc + (N + 1) + (N + 1) + N));
+__host__ __device__ inline size_t sub_bytes(int N, int Mc, bool mixed = false) {
+  return align16(16 * (size_t)(2 * Mc * (mixed ? 2 : 1) + (N + 1) + (N + 1) + N));
 }
 
 __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64_t* g_hx, const uint16_t* g_hxo,
@@ -348,9 +348,17 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 // the tracker kernel
 //   RS  state precision (track, t, dt)      RP  predictor (RK) precision
 //   RCL corrector precision for t < t_switch RCH corrector precision for t >= t_switch
+//
+// Each sub-warp runs its path as a small state machine (phase 0..3 = RK stage,
+// 4 = Newton iteration).  One trip of the warp loop performs exactly one
+// evaluate-and-solve for every sub-warp, whatever its phase, so the unrolled
+// LU exists once per precision in the code and sub-warps of one warp never
+// wait on each other's corrector iterations.
 // -------------------------------------------------------------------------------------------------
 template <typename RS, typename RP, typename RCL, typename RCH, int N, int W, int KIND>
 __global__ void __launch_bounds__(128) track_kernel(const TrackParams p) {
+  static_assert(std::is_same<RP, RCL>::value, "the low-precision corrector shares the predictor's buffers");
+  constexpr bool kMixed = !std::is_same<RCL, RCH>::value;
   extern __shared__ __align__(16) unsigned char smem[];
   const Tables tb = stage_tables(smem, p.hx_terms, p.hx_off, p.ht_terms, p.ht_off, N, p.n_hx_terms, p.n_ht_terms);
 
@@ -358,13 +366,18 @@ __global__ void __launch_bounds__(128) track_kernel(const TrackParams p) {
   const int l = lane % W;
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
-  unsigned char* base = smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc);
-  SubMem sm;
+  unsigned char* base = smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, kMixed);
+  SubMem sm;  // predictor / low-precision corrector buffers
   sm.coefA = base;
   sm.coefB = base + 16 * (size_t)Mc;
   sm.xs = base + 32 * (size_t)Mc;
   sm.sx = sm.xs + 16 * (N + 1);
   sm.sol = sm.sx + 16 * (N + 1);
+  SubMem smh = sm;  // high-precision corrector: own coefficient buffers
+  if (kMixed) {
+    smh.coefA = sm.sol + 16 * N;
+    smh.coefB = smh.coefA + 16 * (size_t)Mc;
+  }
 
   const int subs_per_cta = blockDim.x / W;
   const long long n_sw = (long long)gridDim.x * subs_per_cta;
@@ -375,12 +388,26 @@ __global__ void __launch_bounds__(128) track_kernel(const TrackParams p) {
   bool alive = item < p.n_items;
   long long hyp = 0;
   cx<RS> x = mk(RS(0), RS(0)), x0 = x, sols = x;
-  RS t0 = 0, dt = 0, t_step = 0;
-  bool end_zone = false, success = false, inf = false;
-  int nsucc = 0, step = 0, ncorr = 0;
-
+  RS t0 = 0, dt = 0, t_step = 0, half = 0;
+  bool end_zone = false, success = false, inf = false, hi = false;
+  int nsucc = 0, step = 0, ncorr = 0, phase = 0, cit = 0;
   const RS dt_init = (KIND == KIND_PH) ? RS(0.01) : RS(0.05);
 
+  // end-zone clamp and bookkeeping at the start of a step (kernel_HC_Solver_P3P.cu:121-134)
+  auto prologue = [&]() {
+    if (!end_zone && fabs(f_sub(RS(1), t0)) <= RS(0.0500001)) end_zone = true;
+    if (end_zone) {
+      const RS rem = fabs(f_sub(RS(1), t0));
+      if (dt > rem) dt = rem;
+    } else {
+      const RS edge = (KIND == KIND_PH) ? fabs(f_sub(RS(0.95), t0)) : fabs(f_sub(f_sub(RS(1), RS(0.05)), t0));
+      if (dt > edge) dt = edge;
+    }
+    t_step = t0;
+    half = f_mul(RS(0.5), dt);
+    phase = 0;
+    cit = 0;
+  };
   auto init_path = [&](long long it) {
     hyp = it / p.paths_per_hyp;
     const long long pidx = it % p.paths_per_hyp;
@@ -395,107 +422,83 @@ __global__ void __launch_bounds__(128) track_kernel(const TrackParams p) {
     x0 = x;
     t0 = 0;
     dt = dt_init;
-    t_step = 0;
     end_zone = false;
     success = false;
     inf = false;
     nsucc = 0;
     step = 0;
     ncorr = 0;
+    prologue();
   };
   if (alive) init_path(item);
 
   while (__any_sync(kFull, alive)) {
-    // ---------------- step prologue: end-zone clamp (kernel_HC_Solver_P3P.cu:121-134)
-    RS half = 0;
-    if (alive) {
-      if (!end_zone && fabs(f_sub(RS(1), t0)) <= RS(0.0500001)) end_zone = true;
-      if (end_zone) {
-        const RS rem = fabs(f_sub(RS(1), t0));
-        if (dt > rem) dt = rem;
-      } else {
-        const RS edge = (KIND == KIND_PH) ? fabs(f_sub(RS(0.95), t0)) : fabs(f_sub(f_sub(RS(1), RS(0.05)), t0));
-        if (dt > edge) dt = edge;
-      }
-      t_step = t0;
-      half = f_mul(RS(0.5), dt);
+    const bool rk = alive && phase < 4;
+    const bool corr = alive && phase == 4;
+    // ---------------- coefficients: every RK stage at its t; the corrector reuses stage 4's
+    if (rk) coef_eval<RP, W, KIND>(p, sm, hyp, (RP)t0, l);
+    if (kMixed && corr && cit == 0) {
+      hi = (double)t0 >= p.t_switch;
+      if (hi) coef_eval<RCH, W, KIND>(p, smh, hyp, (RCH)t0, l);
     }
-
-    // ---------------- loopy RK4 predictor (kernel_HC_Solver_P3P.cu:139-183)
-    cx<RS> k = mk(RS(0), RS(0));
-#pragma unroll 1
-    for (int rk = 0; rk < 4; ++rk) {
-      if (alive) coef_eval<RP, W, KIND>(p, sm, hyp, (RP)t0, l);
+    // ---------------- one evaluate-and-solve per sub-warp (predictor: -H_t, corrector: H)
+    const bool use_lo = rk || (corr && !(kMixed && hi));
+    const bool use_hi = kMixed && corr && hi;
+    cx<RS> v = mk(RS(0), RS(0));
+    if (__any_sync(kFull, use_lo)) {
       write_track<RP, RS, N>(sm, l, x);
       __syncwarp(kFull);
-      k = c_cast<RS>(eval_solve<RP, N, W, KIND>(tb, sm, l, 1));
-      if (alive && rk < 3) {
-        const RS a = f_mul(dt, rk == 0 ? RS(1.0 / 6.0) : RS(2.0 / 6.0));
-        const RS d = f_mul(dt, rk == 2 ? RS(1.0) : RS(0.5));
-        sols = mk(f_fma(k.re, a, sols.re), f_fma(k.im, a, sols.im));
-        x = mk(f_fma(k.re, d, x0.re), f_fma(k.im, d, x0.im));
-        if (rk != 1) t0 = f_add(t0, half);
-      }
+      const cx<RS> s = c_cast<RS>(eval_solve<RP, N, W, KIND>(tb, sm, l, rk ? 1 : 0));
+      if (use_lo) v = s;
     }
-    if (alive) {
-      const RS a = f_mul(dt, RS(1.0 / 6.0));
-      sols = mk(f_fma(k.re, a, sols.re), f_fma(k.im, a, sols.im));
-      x = sols;
-    }
-
-    // ---------------- Newton corrector (kernel_HC_Solver_P3P.cu:191-223)
-    const bool hi = !std::is_same<RCL, RCH>::value && alive && ((double)t0 >= p.t_switch);
-    if (!std::is_same<RCH, RP>::value) {
-      if (__any_sync(kFull, hi)) {
-        if (hi) coef_eval<RCH, W, KIND>(p, sm, hyp, (RCH)t0, l);
+    if (kMixed) {
+      if (__any_sync(kFull, use_hi)) {
+        write_track<RCH, RS, N>(smh, l, x);
         __syncwarp(kFull);
+        const cx<RS> s = c_cast<RS>(eval_solve<RCH, N, W, KIND>(tb, smh, l, 0));
+        if (use_hi) v = s;
       }
     }
-    if (!std::is_same<RCL, RP>::value) {
-      if (__any_sync(kFull, alive && !hi)) {
-        if (alive && !hi) coef_eval<RCL, W, KIND>(p, sm, hyp, (RCL)t0, l);
-        __syncwarp(kFull);
-      }
+    // ---------------- corrector norms (kernel_HC_Solver_P3P.cu:204-219), all lanes take part
+    RS ns0 = 0, nc0 = 0;
+    if (__any_sync(kFull, corr)) {
+      const cx<RS> xn = c_sub(x, v);
+      const RS ns = tree_sum<RS, N, W>((corr && l < N) ? c_abs2(v) : RS(0));
+      const RS nc = tree_sum<RS, N, W>((corr && l < N) ? c_abs2(xn) : RS(0));
+      ns0 = __shfl_sync(kFull, ns, leader);
+      nc0 = __shfl_sync(kFull, nc, leader);
     }
-    bool running = alive;
-    success = false;
-    inf = false;
-#pragma unroll 1
-    for (int it = 0; it < p.max_corr; ++it) {
-      if (!__any_sync(kFull, running)) break;
-      // the low- and high-precision sub-warps of this warp (at most two passes)
-#pragma unroll
-      for (int pass = 0; pass < 2; ++pass) {
-        const bool mine = running && (pass == 0 ? !hi : hi);
-        if (pass == 1 && std::is_same<RCL, RCH>::value) break;
-        if (!__any_sync(kFull, mine)) continue;
-        cx<RS> dlt;
-        if (pass == 0) {
-          write_track<RCL, RS, N>(sm, l, x);
-          __syncwarp(kFull);
-          dlt = c_cast<RS>(eval_solve<RCL, N, W, KIND>(tb, sm, l, 0));
-        } else {
-          write_track<RCH, RS, N>(sm, l, x);
-          __syncwarp(kFull);
-          dlt = c_cast<RS>(eval_solve<RCH, N, W, KIND>(tb, sm, l, 0));
-        }
-        if (mine) x = c_sub(x, dlt);
-        const RS ns = tree_sum<RS, N, W>((mine && l < N) ? c_abs2(dlt) : RS(0));
-        const RS nc = tree_sum<RS, N, W>((mine && l < N) ? c_abs2(x) : RS(0));
-        const RS ns0 = __shfl_sync(kFull, ns, leader);
-        const RS nc0 = __shfl_sync(kFull, nc, leader);
-        if (mine) {
-          ++ncorr;
-          success = ((double)ns0 < 1e-6 * (double)nc0);
-          inf = ((double)nc0 > 1e14);
-          if (inf || success) running = false;
-        }
+    // ---------------- per-sub-warp state update (no synchronisation below until the fetch)
+    bool end_step = false;
+    if (rk) {
+      if (phase < 3) {
+        const RS a = f_mul(dt, phase == 0 ? RS(1.0 / 6.0) : RS(2.0 / 6.0));
+        const RS d = f_mul(dt, phase == 2 ? RS(1.0) : RS(0.5));
+        sols = mk(f_fma(v.re, a, sols.re), f_fma(v.im, a, sols.im));
+        x = mk(f_fma(v.re, d, x0.re), f_fma(v.im, d, x0.im));
+        if (phase != 1) t0 = f_add(t0, half);
+        ++phase;
+      } else {
+        const RS a = f_mul(dt, RS(1.0 / 6.0));
+        sols = mk(f_fma(v.re, a, sols.re), f_fma(v.im, a, sols.im));
+        x = sols;
+        phase = 4;
+        cit = 0;
+        success = false;
+        inf = false;
+        if (p.max_corr <= 0) end_step = true;
       }
+    } else if (corr) {
+      x = c_sub(x, v);
+      ++ncorr;
+      ++cit;
+      success = ((double)ns0 < p.corr_tol2 * (double)nc0);
+      inf = ((double)nc0 > 1e14);
+      end_step = inf || success || cit >= p.max_corr || (cit == 1 && (double)ns0 > p.first_tol2 * (double)nc0);
     }
-
-    // ---------------- step control (kernel_HC_Solver_P3P.cu:225-249)
     bool done = false;
-    if (alive) {
+    if (end_step) {
+      // step control (kernel_HC_Solver_P3P.cu:225-249)
       if (inf) {
         done = true;
       } else if (!success) {
@@ -511,14 +514,16 @@ __global__ void __launch_bounds__(128) track_kernel(const TrackParams p) {
         if (nsucc >= p.incr) {
           nsucc = 0;
           dt = f_mul(dt, RS(2));
+          if ((double)dt > p.dt_max) dt = (RS)p.dt_max;
         }
       }
       ++step;
       if (!done) done = !(t0 < RS(1) && f_sub(RS(1), t0) > RS(1e-7)) || step > p.max_steps;
+      if (!done) prologue();
     }
 
     // ---------------- finished paths: write out and take the next path
-    if (alive && done) {
+    if (done) {
       RS* ep = reinterpret_cast<RS*>(p.endpoints) + 2 * item * p.ld_out;
       if (l < N) {
         ep[2 * l] = x.re;
@@ -535,11 +540,10 @@ __global__ void __launch_bounds__(128) track_kernel(const TrackParams p) {
         if (p.dt_end) p.dt_end[item] = (double)dt;
       }
     }
-    const bool need = alive && done;
     long long nxt = 0;
-    if (need && l == 0) nxt = n_sw + (long long)atomicAdd(p.counter, 1);
+    if (done && l == 0) nxt = n_sw + (long long)atomicAdd(p.counter, 1);
     nxt = __shfl_sync(kFull, nxt, leader);
-    if (need) {
+    if (done) {
       item = nxt;
       alive = item < p.n_items;
       if (alive) init_path(item);

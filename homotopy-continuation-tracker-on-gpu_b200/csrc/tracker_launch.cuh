@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "ghc_internal.h"
 #include "tracker.cuh"
 
@@ -16,7 +18,8 @@ int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
   auto kern = dev::track_kernel<RS, RP, RCL, RCH, N, W, KIND>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
-  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc);
+  const bool mixed = !std::is_same<RCL, RCH>::value;
+  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, mixed);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return -20;
   int occ = 0;

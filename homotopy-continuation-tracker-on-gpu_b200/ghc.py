@@ -16,6 +16,10 @@ LIB_PATH = os.path.join(HERE, "libghc_b200.so")
 PROBLEMS = os.path.join(HERE, "problems")
 
 PREC_FP64, PREC_FP32, PREC_MIXED = 0, 1, 2
+
+# Step control without path jumping: tight corrector, contraction test on the
+# first Newton update, bounded step.  Used with a corrector limit of 3.
+ROBUST_STEP = dict(corr_tol2=1e-12, first_tol2=1e-2, dt_max=0.05)
 KIND_P2C, KIND_PH = 0, 1
 STATUS_CONVERGED, STATUS_DIVERGED, STATUS_STEP_CAP = 0, 1, 2
 
@@ -42,6 +46,7 @@ class Counts(ctypes.Structure):
 class TrackArgs(ctypes.Structure):
     _fields_ = [("n_hyp", _I64), ("precision", _I32), ("max_steps", _I32), ("max_corr", _I32),
                 ("incr_steps", _I32), ("t_switch", ctypes.c_double), ("polish_iters", _I32),
+                ("corr_tol2", ctypes.c_double), ("first_tol2", ctypes.c_double), ("dt_max", ctypes.c_double),
                 ("d_start_sols", _P), ("d_coef_hx", _P), ("d_coef_ht", _P), ("d_p_start", _P),
                 ("d_p_target", _P), ("d_p_diff", _P), ("d_endpoints", _P), ("d_status", _P), ("d_conv", _P),
                 ("d_inf", _P), ("d_steps", _P), ("d_corr", _P), ("d_t_end", _P), ("d_dt_end", _P),
@@ -126,7 +131,7 @@ class Problem:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h:
+        if h and ghc_problem_free is not None:
             ghc_problem_free(h)
             self.h = None
 
@@ -189,14 +194,22 @@ class Workspace:
 
 
 def track(pb, ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, d_p_target=None, d_p_diff=None,
-          t_switch=0.9, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False):
-    """Launch the batched tracker (asynchronous on torch's current stream)."""
+          t_switch=0.9, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False, step=None):
+    """Launch the batched tracker (asynchronous on torch's current stream).
+
+    step: optional dict(corr_tol2=, first_tol2=, dt_max=) step control; the
+    default is the reference's (see ROBUST_STEP for the path-jump-free one).
+    """
     a = TrackArgs()
     a.n_hyp = ws.n_hyp
     a.precision = ws.precision
     a.max_steps, a.max_corr, a.incr_steps = max_steps, max_corr, incr_steps
     a.t_switch = t_switch
     a.polish_iters = polish_iters
+    st = step or {}
+    a.corr_tol2 = st.get("corr_tol2", 0.0)
+    a.first_tol2 = st.get("first_tol2", 0.0)
+    a.dt_max = st.get("dt_max", 0.0)
     a.d_start_sols = _ptr(d_start_sols)
     a.d_coef_hx, a.d_coef_ht = _ptr(d_coef_hx), _ptr(d_coef_ht)
     a.d_p_start, a.d_p_target, a.d_p_diff = _ptr(d_p_start), _ptr(d_p_target), _ptr(d_p_diff)

@@ -112,6 +112,10 @@ typedef struct {
   int32_t incr_steps;         /* <= 0: YAML value */
   double t_switch;            /* GHC_PREC_MIXED: FP64 corrector for t >= t_switch */
   int32_t polish_iters;       /* Newton iterations at t = 1 after tracking (FP64 state only) */
+  /* step control; <= 0 selects the reference's value (kernel_HC_Solver_P3P.cu:214) */
+  double corr_tol2;           /* corrector success |dx|^2 < corr_tol2 |x|^2 (reference 1e-6) */
+  double first_tol2;          /* reject a step whose first Newton update has |dx|^2 > first_tol2 |x|^2 (off) */
+  double dt_max;              /* step-size cap (off) */
   /* inputs */
   const void* d_start_sols;   /* [paths][N] complex, state precision (double; float for FP32) */
   const double* d_coef_hx;    /* P2C: [n_hyp][(M+1)(K+1)] complex */

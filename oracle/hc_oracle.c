@@ -34,6 +34,10 @@ typedef struct {
   int32_t polish_iters;
   const int32_t* hx_idx;
   const int32_t* ht_idx;
+  /* step control; the reference's values are corr_tol2 = 1e-6, first_tol2 = inf, dt_max = inf */
+  double corr_tol2;  /* corrector success: |dx|^2 < corr_tol2 * |x|^2 */
+  double first_tol2; /* reject the step when the first Newton update has |dx|^2 > first_tol2 * |x|^2 */
+  double dt_max;     /* upper bound of the step size */
 } orc_problem;
 
 typedef struct {

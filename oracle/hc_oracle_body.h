@@ -338,9 +338,10 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
         nc[r] = SFX(c_abs2)(x[r]);
       }
       const REAL sn = SFX(tree_sum)(ns, N), sc = SFX(tree_sum)(nc, N);
-      success = ((double)sn < 1e-6 * (double)sc);
+      success = ((double)sn < pb->corr_tol2 * (double)sc);
       inf = ((double)sc > 1e14);
       if (inf || success) break;
+      if (it == 0 && (double)sn > pb->first_tol2 * (double)sc) break; /* predictor too far off: reject */
     }
     if (inf) break;
 
@@ -356,6 +357,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
       if (nsucc >= pb->incr_steps) {
         nsucc = 0;
         dt = dt * (REAL)2;
+        if ((double)dt > pb->dt_max) dt = (REAL)pb->dt_max;
       }
     }
   }

@@ -177,7 +177,12 @@ class _Prob(ctypes.Structure):
                 ("Px", ctypes.c_int32), ("Tt", ctypes.c_int32), ("Pt", ctypes.c_int32),
                 ("max_steps", ctypes.c_int32), ("max_corr", ctypes.c_int32),
                 ("incr_steps", ctypes.c_int32), ("polish_iters", ctypes.c_int32),
-                ("hx_idx", ctypes.c_void_p), ("ht_idx", ctypes.c_void_p)]
+                ("hx_idx", ctypes.c_void_p), ("ht_idx", ctypes.c_void_p), ("corr_tol2", ctypes.c_double),
+                ("first_tol2", ctypes.c_double), ("dt_max", ctypes.c_double)]
+
+# step control of the reference (kernel_HC_Solver_P3P.cu:214, no contraction test, no dt cap)
+REFERENCE_STEP = dict(corr_tol2=1e-6, first_tol2=float("inf"), dt_max=float("inf"))
+ROBUST_STEP = dict(corr_tol2=1e-12, first_tol2=1e-2, dt_max=0.05)
 
 
 _LIB = None
@@ -202,7 +207,7 @@ def _cx(a, rt):
     return np.ascontiguousarray(out)
 
 
-def _prob_struct(pb, polish_iters, max_steps=None, max_corr=None, incr=None):
+def _prob_struct(pb, polish_iters, max_steps=None, max_corr=None, incr=None, step=None):
     s = _Prob()
     s.kind, s.N, s.P, s.M, s.K = pb.kind, pb.N, pb.P, pb.M, pb.K
     s.Tx, s.Px, s.Tt, s.Pt = pb.Tx, pb.Px, pb.Tt, pb.Pt
@@ -212,11 +217,14 @@ def _prob_struct(pb, polish_iters, max_steps=None, max_corr=None, incr=None):
     s.polish_iters = polish_iters
     s.hx_idx = pb.hx_idx.ctypes.data
     s.ht_idx = pb.ht_idx.ctypes.data
+    st = dict(REFERENCE_STEP)
+    st.update(step or {})
+    s.corr_tol2, s.first_tol2, s.dt_max = st["corr_tol2"], st["first_tol2"], st["dt_max"]
     return s
 
 
 def track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precision="d",
-          polish_iters=0, nthreads=0, max_steps=None, max_corr=None, incr=None):
+          polish_iters=0, nthreads=0, max_steps=None, max_corr=None, incr=None, step=None):
     """Track all start paths for H hypotheses.
 
     P2C: hx [H, (M+1)(K+1)], ht [H, (M+1)K] complex.
@@ -250,7 +258,7 @@ def track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precisi
     out = dict(conv=np.zeros(n, np.uint8), inf=np.zeros(n, np.uint8), status=np.zeros(n, np.uint8),
                steps=np.zeros(n, np.int32), corr=np.zeros(n, np.int32), t_end=np.zeros(n),
                dt_end=np.zeros(n), resid=np.zeros(n))
-    s = _prob_struct(pb, polish_iters, max_steps, max_corr, incr)
+    s = _prob_struct(pb, polish_iters, max_steps, max_corr, incr, step)
     P = ctypes.c_void_p
 
     def ptr(a):

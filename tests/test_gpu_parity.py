@@ -43,15 +43,20 @@ def inputs(name, n_hyp=1, seed=0):
     return pb, ob, np.array(tg)
 
 
-def run_gpu(pb, ob, targets, precision, polish=0, **kw):
+def run_gpu(pb, ob, targets, precision, polish=0, p2c="oracle", **kw):
     n_hyp = len(targets)
     rt = torch.float32 if precision == ghc.PREC_FP32 else torch.float64
     ws = ghc.Workspace(pb, n_hyp, precision)
     ss = cx_t(ob.start_sols, rt)
     if pb.kind == ghc.KIND_P2C:
-        hx = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[0] for t in targets])
-        ht = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[1] for t in targets])
-        ghc.track(pb, ws, ss, d_coef_hx=cx_t(hx), d_coef_ht=cx_t(ht), polish_iters=polish, **kw)
+        if p2c == "device":
+            dhx, dht = pb.p2c_device(cx_t(ob.start_params), cx_t(targets))
+            hx, ht = to_cx(dhx), to_cx(dht)[:, : (pb.M + 1) * pb.K]
+        else:
+            hx = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[0] for t in targets])
+            ht = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[1] for t in targets])
+            dhx, dht = cx_t(hx), cx_t(ht)
+        ghc.track(pb, ws, ss, d_coef_hx=dhx, d_coef_ht=dht, polish_iters=polish, **kw)
         oargs = dict(hx=hx, ht=ht)
     else:
         ps = cx_t(ob.start_params)
@@ -116,12 +121,34 @@ def test_batched_hypotheses_equal_single_runs(name):
     assert np.array_equal(ws1.steps.cpu().numpy(), ws.steps.cpu().numpy()[2 * n:3 * n])
 
 
-@pytest.mark.parametrize("name", ["generalized_3views_4pts", "5pt_rel_pos_alg_form_quat", "P3P"])
+ROBUST = dict(step=ghc.ROBUST_STEP, max_corr=3, max_steps=2000)
+
+
+@pytest.mark.parametrize("name", ["generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY", "trifocal_2op1p_30x30"])
+def test_fp64_robust_step_bit_exact_vs_oracle(name):
+    pb, ob, tg = inputs(name)
+    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_FP64, polish=2, **ROBUST)
+    r = O.track(ob, ob.start_sols, polish_iters=2, nthreads=NCPU, step=O.ROBUST_STEP, max_corr=3, max_steps=2000,
+                **oargs)
+    compare(ws, r)
+
+
+def real_targets(ob, n_hyp, seed):
+    """real perturbations of the shipped target: real instances have real solutions"""
+    rng = np.random.default_rng(seed)
+    base = ob.target_params[:-1].real
+    return np.array([np.append(base + 0.05 * rng.normal(size=ob.P), 1.0) for _ in range(n_hyp)])
+
+
+@pytest.mark.parametrize("name", ["generalized_3views_4pts", "5pt_rel_pos_alg_form_quat",
+                                  "uncalibrated_trifocal_rel_pos_CY"])
 def test_mixed_precision_recall(name):
-    """FP32 predictor / FP64 end-game: >= 99.5% of the FP64 run's real endpoints found within 1e-8."""
-    pb, ob, tg = inputs(name, n_hyp=2, seed=9)
-    w64, _ = run_gpu(pb, ob, tg, ghc.PREC_FP64, polish=3)
-    wmx, _ = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=3, t_switch=0.9)
+    """FP32 predictor + FP64 corrector, both runs with path-jump-free step control:
+    >= 99.5% of the FP64 run's real endpoints are found by the mixed run within 1e-8."""
+    pb, ob = ghc.Problem(name), O.Problem(name)
+    tg = real_targets(ob, 2, 9)
+    w64, _ = run_gpu(pb, ob, tg, ghc.PREC_FP64, polish=3, **ROBUST)
+    wmx, _ = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=3, t_switch=0.0, **ROBUST)
     e64, emx = to_cx(w64.endpoints), to_cx(wmx.endpoints)
     c64, cmx = w64.conv.cpu().numpy() == 1, wmx.conv.cpu().numpy() == 1
     r64 = w64.resid.cpu().numpy()
@@ -170,7 +197,7 @@ def test_empty_batch_is_a_noop():
 def test_solve_host_end_to_end(name, prec):
     pb, ob, tg = inputs(name)
     out = ghc.solve_host(pb, prec)
-    ws, oargs = run_gpu(pb, ob, tg, prec)
+    ws, oargs = run_gpu(pb, ob, tg, prec, p2c="device")
     assert np.array_equal(out["conv"], ws.conv.cpu().numpy())
     assert np.array_equal(out["endpoints"], to_cx(ws.endpoints))
 
@@ -200,14 +227,19 @@ def test_dropin_reference_abi(name, prec):
     if pb.kind == ghc.KIND_P2C:
         hx, ht = O.p2c_tables(ob.terms, ob.start_params, ob.target_params)
         fn = ghc.ghc_kernel_HC_Solver_P2C if prec == "f" else ghc.ghc_kernel_HC_Solver_P2C_z
+        keep = [cx_t(hx, rt), cx_t(ht, rt)]  # hold the tables alive across the call
         sec = fn(pb.h, st, pb.max_steps, pb.max_corr, pb.incr_steps, p_start.data_ptr(), p_track.data_ptr(),
-                 d_hxi.data_ptr(), d_hti.data_ptr(), cx_t(hx, rt).data_ptr(), cx_t(ht, rt).data_ptr(),
+                 d_hxi.data_ptr(), d_hti.data_ptr(), keep[0].data_ptr(), keep[1].data_ptr(),
                  conv.data_ptr(), inf.data_ptr(), dbg.data_ptr())
         oargs = dict(hx=hx, ht=ht)
     else:
         fn = ghc.ghc_kernel_HC_Solver_PH if prec == "f" else ghc.ghc_kernel_HC_Solver_PH_z
         ps, pt = ob.start_params, ob.target_params
-        keep = [cx_t(ps, rt), cx_t(pt, rt), cx_t(pt - ps, rt)]
+        if prec == "f":  # the FP32 oracle subtracts in float
+            pd = pt.astype(np.complex64) - ps.astype(np.complex64)
+        else:
+            pd = pt - ps
+        keep = [cx_t(ps, rt), cx_t(pt, rt), cx_t(pd, rt)]
         sec = fn(pb.h, st, pb.max_steps, pb.max_corr, pb.incr_steps, p_start.data_ptr(), p_track.data_ptr(),
                  keep[0].data_ptr(), keep[1].data_ptr(), keep[2].data_ptr(), d_hxi.data_ptr(), d_hti.data_ptr(),
                  conv.data_ptr(), inf.data_ptr(), dbg.data_ptr())

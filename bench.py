@@ -1,0 +1,432 @@
+"""Benchmark: hypothesis-solves/s of the batched B200 path tracker.
+
+Workload (one step): H seeded synthetic scenes of the generalized 3-view
+4-point problem (12 unknowns, 583 paths per hypothesis; 3 generalized cameras
+with uniform random rotations and N(0,1) translations, 4 points in [-1,1]^3 at
+depth 4..8, 0.5 px noise at f = 1000) -> per-hypothesis coefficient tables on
+the device -> every path of every hypothesis tracked t: 0 -> 1 in one launch.
+The headline mode is the plain FP64 tracker with the reference's step control
+batched over H hypotheses; it is arithmetically identical, per hypothesis, to
+the single-hypothesis drop-in launch (recall is measured, not assumed).
+Mixed precision and the path-jump-free step control are reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--hyp H] [--impl reference]
+
+N > 1 runs under torchrun: each rank tracks its own H hypotheses (weak
+scaling, no collective on the data path); the elapsed time is the max over
+ranks.  --impl reference times the CPU restatement of the reference tracker
+(the oracle, all host threads) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "homotopy-continuation-tracker-on-gpu_b200")
+sys.path.insert(0, PKG)
+
+PROBLEM = "generalized_3views_4pts"
+METRIC = "hypothesis-solves/s at >=99.5% real-sol recall, mixed vs plain FP64; p50/p99 ms"
+UNIT = "hypotheses/s"
+ROBUST = dict(corr_tol2=1e-12, first_tol2=1e-2, dt_max=0.05)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--hyp", type=int, default=1024)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--quick", action="store_true", help="skip the secondary modes and the CPU baseline")
+    return ap.parse_args()
+
+
+def workload_config(H):
+    return {"workload": "generalized_3views_4pts batched: %d seeded 3-camera scenes x 583 paths per step, "
+                        "plain FP64 tracker, reference step control" % H,
+            "problem": PROBLEM, "unknowns": 12, "paths_per_hypothesis": 583, "hypotheses_per_step": H,
+            "scene": "4 points U[-1,1]^3 at depth 4-8, 3 generalized cameras, 0.5 px noise at f=1000",
+            "l2": "flushed (256 MiB write) before every timed step"}
+
+
+# ----------------------------------------------------------------------------------------------
+# flop model (algorithmic, from the compiled tables; padding terms and the constant slot excluded)
+# ----------------------------------------------------------------------------------------------
+
+def flop_model(pb_raw):
+    """Real flops per RK stage and per corrector iteration of one path."""
+    N, K, M = pb_raw["N"], pb_raw["K"], pb_raw["M"]
+    hx, ht = pb_raw["hx"], pb_raw["ht"]
+    Px, Pt = pb_raw["Px"], pb_raw["Pt"]
+    th = hx.reshape(-1, Px)
+    tt = ht.reshape(-1, Pt)
+    th = th[th[:, 0] != 0]
+    tt = tt[tt[:, 0] != 0]
+    v_hx = (th[:, 2:] != N).sum(axis=1)
+    v_ht = (tt[:, 2:] != N).sum(axis=1)
+    f_hx = float((6 * v_hx + 4).sum())
+    f_h = float((6 * v_ht + 4).sum())
+    f_coef = (M + 1) * 4 * K + (M + 1) * 4 * max(K - 1, 0)
+    f_lu = 8.0 / 3.0 * N ** 3
+    f_solve = 8.0 * N ** 2
+    f_stage = f_coef + f_hx + f_h + f_lu + f_solve + 16 * N
+    f_corr = f_hx + f_h + f_lu + f_solve + 8 * N
+    return f_stage, f_corr
+
+
+# ----------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ----------------------------------------------------------------------------------------------
+
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu, "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------------
+# reference arm: the CPU oracle (restatement of the reference tracker), all host threads
+# ----------------------------------------------------------------------------------------------
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    import scenes
+    ob = O.Problem(PROBLEM)
+    sample = 8
+    cores = os.cpu_count() or 1
+    tg, _ = scenes.generalized_3views_4pts(sample * (args.steps + args.warmup), seed=1000 + args.seed)
+    times = []
+    for s in range(args.warmup + args.steps):
+        hx = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[0] for t in tg[s * sample:(s + 1) * sample]])
+        ht = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[1] for t in tg[s * sample:(s + 1) * sample]])
+        t0 = time.perf_counter()
+        O.track(ob, ob.start_sols, hx=hx, ht=ht, nthreads=cores)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = sample * len(times) / total
+    ms = [1e3 * t for t in times]
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+            "data": "synthetic (seeded scenes)", "config": workload_config(args.hyp),
+            "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "%d hypotheses x 583 paths per step, %d steps" % (sample, len(times))},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    import ghc
+    import scenes
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_mod
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def cx(a, dt=torch.float64):
+        a = np.asarray(a, dtype=np.complex128)
+        return torch.from_numpy(np.ascontiguousarray(np.stack([a.real, a.imag], -1))).to(dt).to(dev)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    H = args.hyp
+    pb = ghc.Problem(PROBLEM)
+    s_host, _ = pb.params()
+    starts = pb.start_sols()
+    tg, _truth = scenes.generalized_3views_4pts(H, seed=args.seed * 7919 + rank)
+    d_start = cx(s_host)
+    d_tg = cx(tg)
+    d_sols = cx(starts)
+    ws = ghc.Workspace(pb, H, ghc.PREC_FP64)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step(ws_, prec, n_hyp=None, targets=None, **kw):
+        hx, ht = pb.p2c_device(d_start, d_tg if targets is None else targets)
+        ghc.track(pb, ws_, d_sols, d_coef_hx=hx, d_coef_ht=ht, **kw)
+        return hx, ht
+
+    # ---------------- warm-up
+    for _ in range(args.warmup):
+        step(ws, ghc.PREC_FP64)
+    barrier()
+
+    # ---------------- timed region: K steps, L2 flushed before each, events on the launching stream
+    step_ms, kern_ms = [], []
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        barrier()
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            k0 = torch.cuda.Event(enable_timing=True)
+            k1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            hx, ht = pb.p2c_device(d_start, d_tg)
+            k0.record(stream)
+            ghc.track(pb, ws, d_sols, d_coef_hx=hx, d_coef_ht=ht)
+            k1.record(stream)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            kern_ms.append(k0.elapsed_time(k1))
+        barrier()
+    total_ms = max_over_ranks(sum(step_ms))
+    n_steps = args.steps
+    value = world * H * n_steps / (total_ms * 1e-3)
+
+    # ---------------- results of the timed batch (last step)
+    steps = ws.steps.cpu().numpy()
+    corr = ws.corr.cpu().numpy()
+    conv = ws.conv.cpu().numpy()
+    ep = ws.endpoints.cpu().numpy()
+    ep = ep[..., 0] + 1j * ep[..., 1]
+
+    # flop model
+    hx_raw, ht_raw = pb.raw_tables()
+    f_stage, f_corr = flop_model(dict(N=pb.N, K=pb.K, M=pb.M, hx=hx_raw, ht=ht_raw, Px=pb.Px, Pt=pb.Pt))
+    flops_launch = 4.0 * steps.sum() * f_stage + corr.sum() * f_corr
+    kern_avg_ms = sum(kern_ms) / len(kern_ms)
+    achieved = flops_launch / (kern_avg_ms * 1e-3) / 1e12
+    peak64 = ghc.measure_fma_peak(ghc.PREC_FP64) / 1e12
+
+    extra = {}
+    if rank == 0:
+        # recall of the batched run vs single-hypothesis drop-in launches of the same hypotheses
+        n_chk = min(H, 16)
+        ws1 = ghc.Workspace(pb, 1, ghc.PREC_FP64)
+        real_b = real_s = match = 0
+        single_ms = []
+        for h in range(n_chk):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            hx1, ht1 = pb.p2c_device(d_start, d_tg[h:h + 1])
+            ghc.track(pb, ws1, d_sols, d_coef_hx=hx1, d_coef_ht=ht1)
+            torch.cuda.synchronize()
+            single_ms.append(1e3 * (time.perf_counter() - t0))
+            e1s = ws1.endpoints.cpu().numpy()
+            e1s = e1s[..., 0] + 1j * e1s[..., 1]
+            c1 = ws1.conv.cpu().numpy() == 1
+            blk = ep[h * pb.paths:(h + 1) * pb.paths]
+            cb = conv[h * pb.paths:(h + 1) * pb.paths] == 1
+            rs = c1 & (np.abs(e1s.imag).max(axis=1) <= 1e-8)
+            real_s += int(rs.sum())
+            for e in e1s[rs]:
+                d = np.abs(blk[cb] - e).max(axis=1) / max(1.0, np.abs(e).max())
+                match += bool(d.size and d.min() <= 1e-8)
+            real_b += int((cb & (np.abs(blk.imag).max(axis=1) <= 1e-8)).sum())
+        extra["recall_vs_single_hypothesis_fp64"] = match / max(1, real_s)
+        extra["dropin_single_hypothesis"] = {"value": 1e3 / statistics.median(single_ms), "unit": UNIT,
+                                             "note": "one hypothesis per launch, median wall ms %.3f"
+                                                     % statistics.median(single_ms)}
+
+        if not args.quick:
+            extra["modes"] = secondary_modes(pb, ghc, cx, d_start, d_sols, scenes, dev, args)
+            # e2e through the C ABI with host buffers (ghc_solve_host: H2D, P2C, track, D2H inside)
+            e2e_ms = []
+            for _ in range(max(2, min(args.steps, 5))):
+                t0 = time.perf_counter()
+                out = ghc.solve_host(pb, ghc.PREC_FP64, targets=tg)
+                e2e_ms.append(1e3 * (time.perf_counter() - t0))
+            h2d = tg.size * 16 + starts.size * 16 + s_host.size * 16
+            d2h = H * pb.paths * (pb.N * 16 + 3 + 4)
+            extra["e2e"] = {"value": H / (statistics.median(e2e_ms) * 1e-3), "unit": UNIT,
+                            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                            "ms_per_step": statistics.median(e2e_ms),
+                            "path": "ghc_solve_host (C ABI, pageable host buffers, synchronous)"}
+            assert np.array_equal(out["conv"], conv), "e2e run differs from the timed run"
+            extra["cpu_baseline"] = cpu_baseline(args)
+    clocks_sum = clocks.summary()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    traffic = None
+    tp = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        t = json.load(open(tp)).get(PROBLEM)
+        if t:
+            traffic = t["bytes_per_path"] * H * pb.paths
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": n_steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / n_steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "complex128", "data": "synthetic (seeded scenes)", "config": workload_config(H),
+        "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+        "recall": extra.get("recall_vs_single_hypothesis_fp64"),
+        "paths": {"per_step": H * pb.paths, "converged_frac": float(conv.mean()), "mean_steps": float(steps.mean()),
+                  "mean_corrector_iters": float(corr.mean())},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                     "frac": achieved / peak64, "traffic": traffic,
+                     "peak_source": "measured FP64 FMA throughput (ghc_measure_fma_peak, burst)",
+                     "kernel_ms": kern_avg_ms, "algorithmic_flop_per_launch": flops_launch},
+        "clocks": clocks_sum,
+        "gpu_launches": 2 * n_steps,
+    }
+    for k in ("e2e", "cpu_baseline", "modes", "dropin_single_hypothesis"):
+        if k in extra:
+            line[k] = extra[k]
+    print(json.dumps(line), flush=True)
+
+
+def secondary_modes(pb, ghc, cx, d_start, d_sols, scenes, dev, args):
+    """Mixed precision and the path-jump-free step control on a smaller batch (one timed step each)."""
+    import torch
+    H2 = min(args.hyp, 256)
+    tg2, _ = scenes.generalized_3views_4pts(H2, seed=4242 + args.seed)
+    d_tg2 = cx(tg2)
+    out = {}
+    runs = {}
+    configs = [("fp64_ref", ghc.PREC_FP64, {}, 0), ("mixed_ref", ghc.PREC_MIXED, dict(t_switch=0.0), 0),
+               ("fp64_robust", ghc.PREC_FP64, dict(step=ROBUST, max_corr=3, max_steps=2000), 3),
+               ("mixed_robust", ghc.PREC_MIXED, dict(step=ROBUST, max_corr=3, max_steps=2000, t_switch=0.0), 3)]
+    for name, prec, kw, pol in configs:
+        ws = ghc.Workspace(pb, H2, prec)
+        hx, ht = pb.p2c_device(d_start, d_tg2)
+        ghc.track(pb, ws, d_sols, d_coef_hx=hx, d_coef_ht=ht, polish_iters=pol, want_resid=True, **kw)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        hx, ht = pb.p2c_device(d_start, d_tg2)
+        ghc.track(pb, ws, d_sols, d_coef_hx=hx, d_coef_ht=ht, polish_iters=pol, want_resid=True, **kw)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        ep = ws.endpoints.cpu().numpy()
+        runs[name] = (ep[..., 0] + 1j * ep[..., 1], ws.conv.cpu().numpy() == 1, ws.resid.cpu().numpy())
+        out[name] = {"value": H2 / (ms * 1e-3), "unit": UNIT, "hypotheses": H2,
+                     "mean_steps": float(ws.steps.float().mean()), "converged_frac": float(ws.conv.float().mean())}
+
+    def recall(ref, cand):
+        e_r, c_r, r_r = runs[ref]
+        e_c, c_c, _ = runs[cand]
+        n = pb.paths
+        real = c_r & (np.abs(e_r.imag).max(axis=1) <= 1e-8)
+        found = 0
+        for i in np.nonzero(real)[0]:
+            h = i // n
+            cand_e = e_c[h * n:(h + 1) * n][c_c[h * n:(h + 1) * n]]
+            d = np.abs(cand_e - e_r[i]).max(axis=1) / max(1.0, np.abs(e_r[i]).max())
+            found += bool(d.size and d.min() <= 1e-8)
+        return found / max(1, int(real.sum()))
+
+    out["mixed_ref"]["recall_vs_fp64_ref"] = recall("fp64_ref", "mixed_ref")
+    out["mixed_robust"]["recall_vs_fp64_robust"] = recall("fp64_robust", "mixed_robust")
+    out["fp64_robust"]["recall_vs_fp64_ref"] = recall("fp64_ref", "fp64_robust")
+    return out
+
+
+def cpu_baseline(args):
+    """The oracle (CPU restatement of the reference tracker) on a bounded sample, all host cores."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    import scenes
+    ob = O.Problem(PROBLEM)
+    cores = os.cpu_count() or 1
+    sample = 8
+    tg, _ = scenes.generalized_3views_4pts(sample, seed=77 + args.seed)
+    hx = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[0] for t in tg])
+    ht = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[1] for t in tg])
+    t0 = time.perf_counter()
+    O.track(ob, ob.start_sols, hx=hx, ht=ht, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": sample / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d hypotheses x 583 paths (same scene generator), FP64, reference step control" % sample}
+
+
+if __name__ == "__main__":
+    main()

@@ -81,6 +81,7 @@ ghc_kernel_HC_Solver_P2C = _sig("ghc_kernel_HC_Solver_P2C", ctypes.c_double, _DR
 ghc_kernel_HC_Solver_P2C_z = _sig("ghc_kernel_HC_Solver_P2C_z", ctypes.c_double, _DROPIN_P2C)
 ghc_kernel_HC_Solver_PH = _sig("ghc_kernel_HC_Solver_PH", ctypes.c_double, _DROPIN_PH)
 ghc_kernel_HC_Solver_PH_z = _sig("ghc_kernel_HC_Solver_PH_z", ctypes.c_double, _DROPIN_PH)
+ghc_measure_fma_peak = _sig("ghc_measure_fma_peak", ctypes.c_int, [ctypes.c_int, _P, _P])
 
 
 class GhcError(RuntimeError):
@@ -220,6 +221,14 @@ def track(pb, ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, 
     a.d_resid = ws.resid.data_ptr() if (want_resid or polish_iters > 0) and ws.precision != PREC_FP32 else None
     a.d_counter = ws.counter.data_ptr()
     _check(ghc_track(pb.h, ctypes.byref(a), _stream()), "ghc_track")
+
+
+def measure_fma_peak(precision=PREC_FP64):
+    """Measured FMA throughput of the current device in FLOP/s."""
+    f = ctypes.c_double()
+    ms = ctypes.c_double()
+    _check(ghc_measure_fma_peak(precision, ctypes.byref(f), ctypes.byref(ms)), "ghc_measure_fma_peak")
+    return f.value
 
 
 def count_results(endpoints, conv, inf, imag_tol=1e-4, dup_tol=1e-4):

@@ -189,6 +189,14 @@ int ghc_solve_host(const ghc_problem* pb, int32_t precision, int64_t n_hyp, cons
                    double t_switch, int32_t polish_iters, double* h_endpoints, uint8_t* h_status, uint8_t* h_conv,
                    uint8_t* h_inf, int32_t* h_steps, double* h_ms);
 
+/* ---------------------------------------------------------------------------
+ * Diagnostics (no counterpart in the reference): measured CUDA-core FMA
+ * throughput of the current device in FLOP/s, the roofline denominator of
+ * the tracker's complex FP64/FP32 arithmetic.  precision: GHC_PREC_FP64 or
+ * GHC_PREC_FP32.  ms (optional): duration of the timed launch.
+ * ------------------------------------------------------------------------- */
+int ghc_measure_fma_peak(int precision, double* flops_per_s, double* ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,7 @@ ghc_problem_raw_tables = _sig("ghc_problem_raw_tables", ctypes.c_int, [_P, _P, _
 ghc_p2c = _sig("ghc_p2c", ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int])
 ghc_p2c_device = _sig("ghc_p2c_device", ctypes.c_int, [_P, _I64, _P, _P, _P, _P, ctypes.c_int, _P])
 ghc_track = _sig("ghc_track", ctypes.c_int, [_P, ctypes.POINTER(TrackArgs), _P])
+ghc_track_noalloc = _sig("ghc_track_noalloc", ctypes.c_int, [_P, ctypes.POINTER(TrackArgs), _P])
 ghc_count_results = _sig("ghc_count_results", ctypes.c_int,
                          [_I32, _I32, _P, _P, _P, ctypes.c_double, ctypes.c_double, ctypes.POINTER(Counts)])
 ghc_solve_host = _sig("ghc_solve_host", ctypes.c_int,
@@ -195,7 +196,8 @@ class Workspace:
 
 
 def track(pb, ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, d_p_target=None, d_p_diff=None,
-          t_switch=0.9, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False, step=None):
+          t_switch=0.9, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False, step=None,
+          no_alloc=False):
     """Launch the batched tracker (asynchronous on torch's current stream).
 
     step: optional dict(corr_tol2=, first_tol2=, dt_max=) step control; the
@@ -220,7 +222,12 @@ def track(pb, ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, 
     a.d_t_end, a.d_dt_end = ws.t_end.data_ptr(), ws.dt_end.data_ptr()
     a.d_resid = ws.resid.data_ptr() if (want_resid or polish_iters > 0) and ws.precision != PREC_FP32 else None
     a.d_counter = ws.counter.data_ptr()
-    _check(ghc_track(pb.h, ctypes.byref(a), _stream()), "ghc_track")
+    if no_alloc:
+        # ghc_track_noalloc: counter and tables in the library's fixed device array
+        a.d_counter = None
+        _check(ghc_track_noalloc(pb.h, ctypes.byref(a), _stream()), "ghc_track_noalloc")
+    else:
+        _check(ghc_track(pb.h, ctypes.byref(a), _stream()), "ghc_track")
 
 
 def measure_fma_peak(precision=PREC_FP64):

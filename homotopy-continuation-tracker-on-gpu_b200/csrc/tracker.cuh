@@ -201,35 +201,36 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
   b = which ? mk(-h.re, -h.im) : h;
 }
 
+// Pivot key of a row for column i: magnitude |Re|+|Im| quantised to its upper
+// bits, position in the low 5 bits (largest key = largest magnitude, lowest
+// position among equal ones).  Pivoted rows 0; NaN at the current position
+// wins, NaN below never does (reference dev-cgesv-batched-small.cuh:54-65).
+__device__ __forceinline__ unsigned mag_bits(double v) { return (unsigned)__double2hiint(v); }
+__device__ __forceinline__ unsigned mag_bits(float v) { return __float_as_uint(v); }
+template <typename R>
+__device__ __forceinline__ unsigned pivot_key(R v, int pos, int i) {
+  if (pos < i) return 0u;
+  if (v != v) return (pos == i) ? 0xffffffffu : 0u;
+  return ((mag_bits(v) >> 5) << 5) | (unsigned)(31 - pos);
+}
+
 // Partial-pivot LU + back substitution, one row per lane, rows in registers.
-// Pivot: max |Re|+|Im| over unpivoted rows, lowest position on ties; NaN at the
-// current position is kept, NaN elsewhere is never chosen (reference
-// dev-cgesv-batched-small.cuh:54-65).  Solution lands in sol[0..N).
-// sx holds N+1 entries (pivot row + its right-hand side).
+// The pivot is found with one warp reduction over the sub-warp's lanes.  A
+// zero pivot skips that column's elimination and leaves a non-finite
+// solution, as in the reference.  Solution lands in sol[0..N); sx holds
+// N+1 entries (pivot row + its right-hand side).
 template <typename R, int N, int W>
 __device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
   const bool live = l < N;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned submask = (W == 32) ? kFull : (((1u << W) - 1u) << (lane & ~(unsigned)(W - 1)));
   int pos = l;
   cx<R> myrcp = mk(R(0), R(0));
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const R v = fabs(A[i].re) + fabs(A[i].im);
-    R key;
-    if (!live || pos < i) key = R(-2);
-    else if (v != v) key = (pos == i) ? (R)CUDART_INF : R(-1);
-    else key = v;
-    R bk = key;
-    int bp = pos;
-#pragma unroll
-    for (int off = W / 2; off > 0; off >>= 1) {
-      const R ok = shfl_xor(bk, off, W);
-      const int op = __shfl_xor_sync(kFull, bp, off, W);
-      if (ok > bk || (ok == bk && op < bp)) {
-        bk = ok;
-        bp = op;
-      }
-    }
-    const bool zero = (bk == R(0));
+    const unsigned key = live ? pivot_key(fabs(A[i].re) + fabs(A[i].im), pos, i) : 0u;
+    const unsigned best = __reduce_max_sync(submask, key);
+    const int bp = 31 - (int)(best & 31u);
     const bool is_piv = live && (pos == bp);
     if (live) {
       if (pos == bp) pos = i;
@@ -237,15 +238,16 @@ __device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* s
     }
     if (is_piv) {
 #pragma unroll
-      for (int j = i; j < N; ++j) sx[j] = zero ? mk(R(0), R(0)) : A[j];
+      for (int j = i; j < N; ++j) sx[j] = A[j];
       sx[N] = b;
     }
     __syncwarp(kFull);
-    const cx<R> rc = c_rcp(sx[i]);
+    const cx<R> p_i = sx[i];
+    const bool zero = (fabs(p_i.re) + fabs(p_i.im) == R(0));
+    const cx<R> rc = c_rcp(zero ? mk(R(0), R(0)) : p_i);
     if (is_piv) myrcp = rc;
-    const cx<R> reg = zero ? mk(R(1), R(0)) : rc;
-    if (live && pos > i) {
-      A[i] = c_mul(A[i], reg);
+    if (live && pos > i && !zero) {
+      A[i] = c_mul(A[i], rc);
 #pragma unroll
       for (int j = i + 1; j < N; ++j) A[j] = c_fnma(A[i], sx[j], A[j]);
       b = c_fnma(A[i], sx[N], b);
@@ -355,8 +357,11 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 // LU exists once per precision in the code and sub-warps of one warp never
 // wait on each other's corrector iterations.
 // -------------------------------------------------------------------------------------------------
+#ifndef GHC_TRACK_MIN_BLOCKS
+#define GHC_TRACK_MIN_BLOCKS 1
+#endif
 template <typename RS, typename RP, typename RCL, typename RCH, int N, int W, int KIND>
-__global__ void __launch_bounds__(128) track_kernel(const TrackParams p) {
+__global__ void __launch_bounds__(128, GHC_TRACK_MIN_BLOCKS) track_kernel(const TrackParams p) {
   static_assert(std::is_same<RP, RCL>::value, "the low-precision corrector shares the predictor's buffers");
   constexpr bool kMixed = !std::is_same<RCL, RCH>::value;
   extern __shared__ __align__(16) unsigned char smem[];

@@ -32,7 +32,9 @@
  *   - padding terms (integer scale 0) are skipped and variable slot N (the
  *     constant 1) is not multiplied in;
  *   - the pivot reciprocal is conj(b)/|b|^2 (one reciprocal); the back
- *     substitution multiplies by the reciprocal formed during elimination.
+ *     substitution multiplies by the reciprocal formed during elimination;
+ *   - pivot magnitudes are compared after quantisation to their upper bits
+ *     (pivot_key), ties going to the lowest position.
  */
 
 #define CAT2(a, b) a##b
@@ -198,12 +200,34 @@ static CX SFX(eval_h_row)(const orc_problem* pb, const COEFS* cf, const CX* x, i
 }
 
 /*
+ * Pivot key of one row for column i: the magnitude |Re|+|Im| quantised to its
+ * upper bits with the position in the low 5 bits, so the largest key is the
+ * largest magnitude and, among magnitudes equal after quantisation, the
+ * lowest position.  Pivoted rows get 0; a NaN at the current position gets the
+ * maximum (the reference keeps position i when its value is NaN), NaN below
+ * never wins (its comparisons are false in the reference's scan).
+ */
+static inline uint32_t SFX(pivot_key)(REAL v, int pos, int i) {
+  if (pos < i) return 0u;
+  if (v != v) return (pos == i) ? 0xffffffffu : 0u;
+  uint32_t hi;
+  if (sizeof(REAL) == 8) {
+    double d = (double)v;
+    uint64_t b;
+    memcpy(&b, &d, 8);
+    hi = (uint32_t)(b >> 32);
+  } else {
+    float f = (float)v;
+    memcpy(&hi, &f, 4);
+  }
+  return ((hi >> 5) << 5) | (uint32_t)(31 - pos);
+}
+
+/*
  * Solve A z = b with partial pivoting, one row per (virtual) lane.
- * Pivot: largest |Re|+|Im| among not-yet-pivoted rows, lowest position on
- * ties; a NaN at position i keeps position i, NaNs elsewhere are never chosen
- * (the sequential strict-> scan of the reference).  A zero pivot skips the
- * elimination for that column and leaves a non-finite solution, as in the
- * reference.  The solution is returned in variable order in z.
+ * Pivot: the row with the largest pivot_key among not-yet-pivoted rows.  A
+ * zero pivot skips the elimination for that column and leaves a non-finite
+ * solution, as in the reference.  The solution is returned in variable order.
  */
 static void SFX(lu_solve)(int N, CX A[][ORC_NMAX], CX* b, CX* z) {
   int pos[ORC_NMAX];
@@ -211,34 +235,31 @@ static void SFX(lu_solve)(int N, CX A[][ORC_NMAX], CX* b, CX* z) {
   for (int r = 0; r < N; ++r) pos[r] = r;
   for (int i = 0; i < N; ++i) {
     int best_r = -1;
-    REAL best_key = 0;
-    int best_pos = 0;
+    uint32_t best_key = 0;
     for (int r = 0; r < N; ++r) {
-      REAL v = FABS(A[r][i].re) + FABS(A[r][i].im);
-      REAL key;
-      if (pos[r] < i) key = (REAL)-2;
-      else if (v != v) key = (pos[r] == i) ? (REAL)INFINITY : (REAL)-1;
-      else key = v;
-      if (best_r < 0 || key > best_key || (key == best_key && pos[r] < best_pos)) {
+      const uint32_t key = SFX(pivot_key)(FABS(A[r][i].re) + FABS(A[r][i].im), pos[r], i);
+      if (best_r < 0 || key > best_key) {
         best_r = r;
         best_key = key;
-        best_pos = pos[r];
       }
     }
-    const int zero = (best_key == (REAL)0);
-    /* swap positions */
+    const int best_pos = 31 - (int)(best_key & 31u);
+    for (int r = 0; r < N; ++r)
+      if (pos[r] == best_pos) best_r = r;
+    /* zero pivot: the pivot row's own magnitude is exactly 0 */
+    const int zero = (FABS(A[best_r][i].re) + FABS(A[best_r][i].im) == (REAL)0);
     for (int r = 0; r < N; ++r)
       if (r != best_r && pos[r] == i) pos[r] = best_pos;
     pos[best_r] = i;
     CX sx[ORC_NMAX];
-    for (int j = i; j < N; ++j) sx[j] = zero ? SFX(c_make)(0, 0) : A[best_r][j];
+    for (int j = i; j < N; ++j) sx[j] = A[best_r][j];
     const CX sb = b[best_r];
-    const CX rc = SFX(c_rcp)(sx[i]);
+    const CX rc = SFX(c_rcp)(zero ? SFX(c_make)(0, 0) : sx[i]);
     myrcp[best_r] = rc;
-    const CX reg = zero ? SFX(c_make)(1, 0) : rc;
+    if (zero) continue; /* zero pivot: no elimination in this column */
     for (int r = 0; r < N; ++r) {
       if (pos[r] > i) {
-        A[r][i] = SFX(c_mul)(A[r][i], reg);
+        A[r][i] = SFX(c_mul)(A[r][i], rc);
         for (int j = i + 1; j < N; ++j) A[r][j] = SFX(c_fnma)(A[r][i], sx[j], A[r][j]);
         b[r] = SFX(c_fnma)(A[r][i], sb, b[r]);
       }

@@ -215,21 +215,20 @@ __device__ __forceinline__ unsigned pivot_key(R v, int pos, int i) {
 }
 
 // Partial-pivot LU + back substitution, one row per lane, rows in registers.
-// The pivot is found with one warp reduction over the sub-warp's lanes.  A
+// The pivot is found by an integer max butterfly over the sub-warp.  A
 // zero pivot skips that column's elimination and leaves a non-finite
 // solution, as in the reference.  Solution lands in sol[0..N); sx holds
 // N+1 entries (pivot row + its right-hand side).
 template <typename R, int N, int W>
 __device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
   const bool live = l < N;
-  const unsigned lane = threadIdx.x & 31u;
-  const unsigned submask = (W == 32) ? kFull : (((1u << W) - 1u) << (lane & ~(unsigned)(W - 1)));
   int pos = l;
   cx<R> myrcp = mk(R(0), R(0));
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const unsigned key = live ? pivot_key(fabs(A[i].re) + fabs(A[i].im), pos, i) : 0u;
-    const unsigned best = __reduce_max_sync(submask, key);
+    unsigned best = live ? pivot_key(fabs(A[i].re) + fabs(A[i].im), pos, i) : 0u;
+#pragma unroll
+    for (int off = W / 2; off > 0; off >>= 1) best = max(best, __shfl_xor_sync(kFull, best, off, W));
     const int bp = 31 - (int)(best & 31u);
     const bool is_piv = live && (pos == bp);
     if (live) {
@@ -322,8 +321,19 @@ __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t
 __host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
   return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(N * N + 1 + N + 1));
 }
-__host__ __device__ inline size_t sub_bytes(int N, int Mc, bool mixed = false) {
-  return align16(16 * (size_t)(2 * Mc * (mixed ? 2 : 1) + (N + 1) + (N + 1) + N));
+__host__ __device__ inline size_t sub_bytes(int N, int Mc, bool mixed = false, int W = 0) {
+  return align16(16 * (size_t)(2 * Mc * (mixed ? 2 : 1) + (N + 1) + (N + 1) + N + 2 * W));
+}
+
+// CTAs per SM the tracker asks the register allocator for: the row of H_x (N
+// complex values) dominates the registers, so small systems afford more.
+// Measured on B200 (FP64): N = 3 best at 8, N = 6 at 4, N = 12 at 6; mixed N = 12 at 4.
+template <int N, typename RS, typename RP>
+constexpr int track_min_blocks() {
+  return (sizeof(RS) == 8 && sizeof(RP) == 8)
+             ? (N <= 4 ? 8 : N <= 8 ? 4 : N <= 12 ? 6 : N <= 18 ? 3 : 2)
+             : (sizeof(RS) == 8 ? (N <= 4 ? 8 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
+                                : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 3));
 }
 
 __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64_t* g_hx, const uint16_t* g_hxo,
@@ -357,11 +367,13 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 // LU exists once per precision in the code and sub-warps of one warp never
 // wait on each other's corrector iterations.
 // -------------------------------------------------------------------------------------------------
-#ifndef GHC_TRACK_MIN_BLOCKS
-#define GHC_TRACK_MIN_BLOCKS 1
+#ifdef GHC_TRACK_MIN_BLOCKS
+#define GHC_MINB(N, RS, RP) GHC_TRACK_MIN_BLOCKS
+#else
+#define GHC_MINB(N, RS, RP) track_min_blocks<N, RS, RP>()
 #endif
 template <typename RS, typename RP, typename RCL, typename RCH, int N, int W, int KIND>
-__global__ void __launch_bounds__(128, GHC_TRACK_MIN_BLOCKS) track_kernel(const TrackParams p) {
+__global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const TrackParams p) {
   static_assert(std::is_same<RP, RCL>::value, "the low-precision corrector shares the predictor's buffers");
   constexpr bool kMixed = !std::is_same<RCL, RCH>::value;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -371,7 +383,7 @@ __global__ void __launch_bounds__(128, GHC_TRACK_MIN_BLOCKS) track_kernel(const 
   const int l = lane % W;
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
-  unsigned char* base = smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, kMixed);
+  unsigned char* base = smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, kMixed, W);
   SubMem sm;  // predictor / low-precision corrector buffers
   sm.coefA = base;
   sm.coefB = base + 16 * (size_t)Mc;
@@ -383,6 +395,10 @@ __global__ void __launch_bounds__(128, GHC_TRACK_MIN_BLOCKS) track_kernel(const 
     smh.coefA = sm.sol + 16 * N;
     smh.coefB = smh.coefA + 16 * (size_t)Mc;
   }
+  // this lane's RK base point x0 and accumulator sols live in shared memory (register relief)
+  unsigned char* lane_state = (kMixed ? smh.coefB + 16 * (size_t)Mc : sm.sol + 16 * N) + 16 * (size_t)l;
+  cx<RS>& x0 = *reinterpret_cast<cx<RS>*>(lane_state);
+  cx<RS>& sols = *reinterpret_cast<cx<RS>*>(lane_state + 16 * W);
 
   const int subs_per_cta = blockDim.x / W;
   const long long n_sw = (long long)gridDim.x * subs_per_cta;
@@ -392,7 +408,7 @@ __global__ void __launch_bounds__(128, GHC_TRACK_MIN_BLOCKS) track_kernel(const 
   long long item = (long long)blockIdx.x * subs_per_cta + g;
   bool alive = item < p.n_items;
   long long hyp = 0;
-  cx<RS> x = mk(RS(0), RS(0)), x0 = x, sols = x;
+  cx<RS> x = mk(RS(0), RS(0));
   RS t0 = 0, dt = 0, t_step = 0, half = 0;
   bool end_zone = false, success = false, inf = false, hi = false;
   int nsucc = 0, step = 0, ncorr = 0, phase = 0, cit = 0;

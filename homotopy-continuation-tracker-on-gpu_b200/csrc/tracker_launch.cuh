@@ -19,7 +19,7 @@ int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
   const bool mixed = !std::is_same<RCL, RCH>::value;
-  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, mixed);
+  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, mixed, W);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return -20;
   int occ = 0;

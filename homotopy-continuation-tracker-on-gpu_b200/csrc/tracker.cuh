@@ -454,31 +454,27 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
   if (alive) init_path(item);
 
   while (__any_sync(kFull, alive)) {
-    const bool rk = alive && phase < 4;
-    const bool corr = alive && phase == 4;
+    // ---------------- which sub-warps are served this trip.  Mixed precision: one precision per
+    // trip for the whole warp (the high-precision corrector first); the others wait one trip.
+    const bool want_hi = kMixed && alive && phase == 4 && hi;
+    const bool want_lo = alive && !want_hi;
+    const bool serve_hi = kMixed && __any_sync(kFull, want_hi);
+    const bool served = serve_hi ? want_hi : want_lo;
+    const bool rk = served && phase < 4;
+    const bool corr = served && phase == 4;
     // ---------------- coefficients: every RK stage at its t; the corrector reuses stage 4's
     if (rk) coef_eval<RP, W, KIND>(p, sm, hyp, (RP)t0, l);
-    if (kMixed && corr && cit == 0) {
-      hi = (double)t0 >= p.t_switch;
-      if (hi) coef_eval<RCH, W, KIND>(p, smh, hyp, (RCH)t0, l);
-    }
-    // ---------------- one evaluate-and-solve per sub-warp (predictor: -H_t, corrector: H)
-    const bool use_lo = rk || (corr && !(kMixed && hi));
-    const bool use_hi = kMixed && corr && hi;
+    if (kMixed && corr && hi && cit == 0) coef_eval<RCH, W, KIND>(p, smh, hyp, (RCH)t0, l);
+    // ---------------- one evaluate-and-solve per served sub-warp (predictor: -H_t, corrector: H)
     cx<RS> v = mk(RS(0), RS(0));
-    if (__any_sync(kFull, use_lo)) {
+    if (!serve_hi) {
       write_track<RP, RS, N>(sm, l, x);
       __syncwarp(kFull);
-      const cx<RS> s = c_cast<RS>(eval_solve<RP, N, W, KIND>(tb, sm, l, rk ? 1 : 0));
-      if (use_lo) v = s;
-    }
-    if (kMixed) {
-      if (__any_sync(kFull, use_hi)) {
-        write_track<RCH, RS, N>(smh, l, x);
-        __syncwarp(kFull);
-        const cx<RS> s = c_cast<RS>(eval_solve<RCH, N, W, KIND>(tb, smh, l, 0));
-        if (use_hi) v = s;
-      }
+      v = c_cast<RS>(eval_solve<RP, N, W, KIND>(tb, sm, l, rk ? 1 : 0));
+    } else if (kMixed) {
+      write_track<RCH, RS, N>(smh, l, x);
+      __syncwarp(kFull);
+      v = c_cast<RS>(eval_solve<RCH, N, W, KIND>(tb, smh, l, 0));
     }
     // ---------------- corrector norms (kernel_HC_Solver_P3P.cu:204-219), all lanes take part
     RS ns0 = 0, nc0 = 0;
@@ -505,6 +501,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
         x = sols;
         phase = 4;
         cit = 0;
+        hi = kMixed && (double)t0 >= p.t_switch;
         success = false;
         inf = false;
         if (p.max_corr <= 0) end_step = true;

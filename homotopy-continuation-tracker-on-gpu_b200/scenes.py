@@ -71,6 +71,38 @@ def generalized_3views_4pts(n_hyp, seed=0, noise_px=0.5, focal=1000.0, offset_sc
     return targets, truth
 
 
+def p3p_td(n_hyp, seed=0):
+    """P3P by a total-degree homotopy (problem P3P_TD, 12 parameters, 3 unknowns).
+
+    Returns ((start [P+1], targets [H, P+1]), truth [H, 3]).  One seeded
+    unit-modulus gamma per call (the start system gamma (x_k^2 - 1)); per
+    hypothesis three points uniform in [-1,1]^3 at depth 4..8 seen from the
+    origin: bearings b_i = X_i / |X_i|, c_ij = b_i . b_j, s_ij = |X_i - X_j|^2;
+    the true depths |X_i| are a real root of the target system.
+    """
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "gen"))
+    import make_p3p_td as m
+    rng = np.random.default_rng(seed)
+    gamma = np.exp(1j * rng.uniform(0.0, 2 * np.pi))
+    start = np.append(np.array(m.start_params(gamma), dtype=np.complex128), 1.0)
+    targets = np.zeros((n_hyp, 13), dtype=np.complex128)
+    truth = np.zeros((n_hyp, 3))
+    for h in range(n_hyp):
+        X = rng.uniform(-1, 1, size=(3, 3))
+        X[:, 2] += rng.uniform(4, 8, size=3)
+        d = np.linalg.norm(X, axis=1)
+        b = X / d[:, None]
+        c = {(i, j): float(b[i] @ b[j]) for (i, j) in m.PAIRS}
+        s2 = {(i, j): float(np.sum((X[i] - X[j]) ** 2)) for (i, j) in m.PAIRS}
+        targets[h, :12] = m.target_params(c, s2)
+        targets[h, 12] = 1.0
+        truth[h] = d
+    return (start, targets), truth
+
+
 GENERATORS = {
     "generalized_3views_4pts": generalized_3views_4pts,
+    "P3P_TD": p3p_td,
 }

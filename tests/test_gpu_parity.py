@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 SUPPORTED = ["P3P", "5pt_rel_pos_alg_form_quat", "generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY",
              "3view_triangulation", "6pt_RS_abs_pos", "dual_reciever_TDOA_5pt", "distorted_2view_triangulation",
-             "P3P_10x10", "trifocal_2op1p_30x30"]
+             "P3P_10x10", "trifocal_2op1p_30x30", "P3P_TD"]
 NCPU = os.cpu_count() or 1
 
 

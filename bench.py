@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--quick", action="store_true", help="skip the secondary modes and the CPU baseline")
+    ap.add_argument("--config", default="g3v4", choices=["g3v4", "cy", "p3p_td", "mix", "served", "g3v4_mono"],
+                    help="g3v4: the headline (default); the others are the remaining workloads of the scope")
     return ap.parse_args()
 
 
@@ -189,6 +191,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank)
+        return
+    if args.config != "g3v4":
+        import workloads
+        workloads.run(args)
         return
 
     import torch

@@ -393,8 +393,8 @@ int ghc_track(const ghc_problem* h, const ghc_track_args* a, void* stream) {
   if (a->max_steps > 0) p.max_steps = a->max_steps;
   if (a->max_corr > 0) p.max_corr = a->max_corr;
   if (a->incr_steps > 0) p.incr = a->incr_steps;
-  p.n_items = a->n_hyp * (long long)pb.paths;
-  p.paths_per_hyp = pb.paths;
+  p.n_items = a->n_hyp * (long long)(a->paths > 0 ? a->paths : pb.paths);
+  p.paths_per_hyp = a->paths > 0 ? a->paths : pb.paths;
   p.start_sols = a->d_start_sols;
   p.ld_start = pb.N;
   p.track_in = nullptr;

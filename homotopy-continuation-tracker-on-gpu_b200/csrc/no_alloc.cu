@@ -134,8 +134,8 @@ extern "C" int ghc_track_noalloc(const ghc_problem* h, const ghc_track_args* a, 
   p.hx_off = reinterpret_cast<const uint16_t*>(s + o_hxo);
   p.ht_terms = reinterpret_cast<const uint64_t*>(s + o_ht);
   p.ht_off = reinterpret_cast<const uint16_t*>(s + o_hto);
-  p.n_items = a->n_hyp * (long long)pb.paths;
-  p.paths_per_hyp = pb.paths;
+  p.n_items = a->n_hyp * (long long)(a->paths > 0 ? a->paths : pb.paths);
+  p.paths_per_hyp = a->paths > 0 ? a->paths : pb.paths;
   p.start_sols = a->d_start_sols;
   p.ld_start = pb.N;
   p.ld_track = pb.N;

@@ -50,7 +50,7 @@ class TrackArgs(ctypes.Structure):
                 ("d_start_sols", _P), ("d_coef_hx", _P), ("d_coef_ht", _P), ("d_p_start", _P),
                 ("d_p_target", _P), ("d_p_diff", _P), ("d_endpoints", _P), ("d_status", _P), ("d_conv", _P),
                 ("d_inf", _P), ("d_steps", _P), ("d_corr", _P), ("d_t_end", _P), ("d_dt_end", _P),
-                ("d_resid", _P), ("d_counter", _P)]
+                ("d_resid", _P), ("d_counter", _P), ("paths", _I32)]
 
 
 def _sig(name, res, args):
@@ -177,9 +177,10 @@ class Problem:
 class Workspace:
     """Device output buffers for ``track`` (reused across calls)."""
 
-    def __init__(self, pb, n_hyp, precision, device="cuda"):
+    def __init__(self, pb, n_hyp, precision, device="cuda", paths=None):
         import torch
-        n = n_hyp * pb.paths
+        self.paths = pb.paths if paths is None else paths
+        n = n_hyp * self.paths
         rt = torch.float32 if precision == PREC_FP32 else torch.float64
         self.n_hyp = n_hyp
         self.precision = precision
@@ -222,6 +223,7 @@ def track(pb, ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, 
     a.d_t_end, a.d_dt_end = ws.t_end.data_ptr(), ws.dt_end.data_ptr()
     a.d_resid = ws.resid.data_ptr() if (want_resid or polish_iters > 0) and ws.precision != PREC_FP32 else None
     a.d_counter = ws.counter.data_ptr()
+    a.paths = ws.paths
     if no_alloc:
         # ghc_track_noalloc: counter and tables in the library's fixed device array
         a.d_counter = None

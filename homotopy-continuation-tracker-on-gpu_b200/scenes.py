@@ -102,7 +102,141 @@ def p3p_td(n_hyp, seed=0):
     return (start, targets), truth
 
 
+def small_rotation(rng, max_angle):
+    """Rotation about a uniform random axis by an angle uniform in [0, max_angle]."""
+    k = rng.normal(size=3)
+    k /= np.linalg.norm(k)
+    a = rng.uniform(0, max_angle)
+    K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+    return np.eye(3) + np.sin(a) * K + (1 - np.cos(a)) * (K @ K)
+
+
+def uncalibrated_trifocal_rel_pos_CY(n_hyp, seed=0, noise_px=0.5, outlier_frac=0.3, image_px=1000.0):
+    """Trifocal relative pose with an unknown shared focal length (24 parameters, 12 unknowns).
+
+    The system (auto-data-gen-tools/p2c-problems/sys_uncalibrated_trifocal_rel_pos_CY.m)
+    equates, for every pair of the 4 points, their distance seen in camera 1
+    with camera 2 (f1-f6) and camera 3 (f7-f12), on rays m = (u, v, sqrt(x1)):
+        | x_b m_b - x_a m_a |_cam1 = | x_{4+a} n_a - x_{4+b} n_b |_cam2 ...
+    Parameters: p1..p4 / p5..p8 the u / v image coordinates of points 1..4 in
+    camera 1, p9..p16 in camera 2, p17..p24 in camera 3 (principal point at
+    0, units of image_px pixels).  Unknowns: x1 = f^2, x2..x4 the camera-1
+    depths of points 2..4 relative to point 1, x5..x8 and x9..x12 the depths
+    of points 1..4 in cameras 2 and 3 relative to the same.
+    A hypothesis is a minimal sample: each of the 4 correspondences is, with
+    probability outlier_frac, replaced in cameras 2 and 3 by a random image
+    point.  truth[h] holds the scene's unknowns (meaningful for inlier samples);
+    inlier[h] tells which hypotheses are all-inlier.
+    """
+    rng = np.random.default_rng(seed)
+    P = 24
+    targets = np.zeros((n_hyp, P + 1), dtype=np.complex128)
+    truth = np.zeros((n_hyp, 12))
+    inlier = np.zeros(n_hyp, dtype=bool)
+    sigma = noise_px / image_px
+    for h in range(n_hyp):
+        while True:
+            f = rng.uniform(0.8, 1.2)
+            X = rng.uniform(-1, 1, size=(4, 3))
+            X[:, 2] += rng.uniform(4, 8, size=4)
+            uv = np.zeros((3, 4, 2))
+            z = np.zeros((3, 4))
+            ok = True
+            for j in range(3):
+                R = small_rotation(rng, 0.3) if j > 0 else np.eye(3)
+                t = 0.5 * rng.normal(size=3) if j > 0 else np.zeros(3)
+                Y = X @ R.T + t
+                if np.any(Y[:, 2] < 1.0):
+                    ok = False
+                z[j] = Y[:, 2]
+                uv[j] = f * Y[:, :2] / Y[:, 2:3] + sigma * rng.normal(size=(4, 2))
+            if ok:
+                break
+        out = rng.random(4) < outlier_frac
+        for i in np.nonzero(out)[0]:
+            for j in (1, 2):
+                uv[j, i] = rng.uniform(-0.5, 0.5, size=2)
+        inlier[h] = not out.any()
+        p = np.concatenate([uv[0, :, 0], uv[0, :, 1], uv[1, :, 0], uv[1, :, 1], uv[2, :, 0], uv[2, :, 1]])
+        targets[h, :P] = p
+        targets[h, P] = 1.0
+        truth[h] = np.concatenate([[f * f], z[0, 1:] / z[0, 0], z[1] / z[0, 0], z[2] / z[0, 0]])
+    return targets, truth, inlier
+
+
+def complex_orthogonal(rng, n=3):
+    """Random complex matrix with R^T R = I (Cayley transform of a complex skew matrix)."""
+    a = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    S = 0.5 * (a - a.T)
+    I = np.eye(n)
+    return np.linalg.solve(I - S, I + S)
+
+
+def seed_pair(name, seed=0):
+    """A generic complex (solution, parameters) pair with F(x; p) = 0, for monodromy.
+
+    generalized_3views_4pts: a complexified scene -- complex points, complex
+    orthogonal camera rotations, complex translations and ray offsets; the
+    equations only use bilinear dot products, so the depth identities hold.
+    P3P: complex bearings b_i and depths x_i with world points X_i = x_i b_i.
+    Returns (x [N] complex, p [P+1] complex with p[P] = 1).
+    """
+    rng = np.random.default_rng(seed)
+    cn = lambda *shape: rng.normal(size=shape) + 1j * rng.normal(size=shape)  # noqa: E731
+    if name == "generalized_3views_4pts":
+        X = cn(4, 3)
+        c1 = cn(4, 3) * 0.3
+        c1[0] = 0.0
+        dirs = np.zeros((3, 4, 3), dtype=complex)
+        depth = np.zeros((3, 4), dtype=complex)
+        for j in range(3):
+            R = complex_orthogonal(rng) if j > 0 else np.eye(3)
+            t = cn(3) if j > 0 else np.zeros(3)
+            o1 = cn(3) * 0.3
+            for i in range(4):
+                Y = R @ X[i] + t - (o1 - c1[i])
+                depth[j, i] = Y[2]
+                dirs[j, i] = Y / Y[2]
+        p = np.concatenate([dirs[0].reshape(-1), dirs[1].reshape(-1), dirs[2].reshape(-1), c1[1], c1[2], c1[3], [1.0]])
+        return np.concatenate([depth[0], depth[1], depth[2]]), p
+    if name == "P3P":
+        b = cn(3, 3)
+        x = cn(3)
+        X = x[:, None] * b
+        return x, np.concatenate([b.reshape(-1), X.reshape(-1), [1.0]])
+    raise KeyError(name)
+
+
+def perturbed_targets(target, n_hyp, seed=0, scale=0.05):
+    """Seeded real perturbations of a problem's shipped target parameters (slot P kept at 1).
+
+    Stands in for scene generators not written here (5-point relative pose,
+    trifocal 30x30 from lines): real instances near the shipped one.
+    """
+    rng = np.random.default_rng(seed)
+    base = np.asarray(target, dtype=np.complex128)[:-1].real
+    out = np.empty((n_hyp, base.size + 1), dtype=np.complex128)
+    out[:, :-1] = base[None, :] + scale * rng.normal(size=(n_hyp, base.size))
+    out[:, -1] = 1.0
+    return out
+
+
+def targets_for(name, n_hyp, seed, start, shipped_target):
+    """(start params [P+1], targets [H, P+1], truth or None) for a problem's batch."""
+    if name == "generalized_3views_4pts":
+        tg, truth = generalized_3views_4pts(n_hyp, seed=seed)
+        return start, tg, truth
+    if name == "uncalibrated_trifocal_rel_pos_CY":
+        tg, truth, _ = uncalibrated_trifocal_rel_pos_CY(n_hyp, seed=seed)
+        return start, tg, truth
+    if name == "P3P_TD":
+        (st, tg), truth = p3p_td(n_hyp, seed=seed)
+        return st, tg, truth
+    return start, perturbed_targets(shipped_target, n_hyp, seed=seed), None
+
+
 GENERATORS = {
     "generalized_3views_4pts": generalized_3views_4pts,
+    "uncalibrated_trifocal_rel_pos_CY": uncalibrated_trifocal_rel_pos_CY,
     "P3P_TD": p3p_td,
 }

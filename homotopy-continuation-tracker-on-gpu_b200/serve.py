@@ -1,0 +1,243 @@
+"""Serving loop: continuous batching of tracking requests of mixed problems.
+
+A request is (problem, target parameters of n hypotheses).  The server keeps
+per problem a CUDA stream and two buffer slots (targets, coefficient tables,
+endpoints and flags for up to ``capacity`` hypotheses), sized at start-up from
+the free device memory (``admission``: the budget is split evenly over the
+problems and slots, capped at ``max_batch`` hypotheses per launch).
+
+The loop admits every request that has arrived into its problem's queue;
+whenever a slot of that problem is free it packs the queued requests (FIFO,
+whole requests, up to the slot's capacity) into one batch, copies the targets
+from pinned host memory, builds the coefficient tables on the device and
+launches the tracker on the problem's stream -- while batches of the other
+problems (and the other slot of the same problem) are still running.  When a
+batch's event has completed, each request's slice of the endpoints and flags
+is copied back and the request is complete.  Results do not depend on which
+other requests shared a launch: every hypothesis is tracked with the same
+arithmetic alone or in a batch (tests/test_gpu_serve.py checks this).
+
+``sequential=True`` gives the baseline of the same GPU without batching: one
+request per launch, one stream, FIFO.
+"""
+import collections
+import json
+import time
+
+import numpy as np
+
+import ghc
+import scenes
+
+MIX = ["P3P_TD", "5pt_rel_pos_alg_form_quat", "generalized_3views_4pts", "trifocal_2op1p_30x30"]
+
+
+class Request:
+    __slots__ = ("rid", "problem", "targets", "arrival", "done", "endpoints", "conv", "status")
+
+    def __init__(self, rid, problem, targets, arrival):
+        self.rid, self.problem, self.targets, self.arrival = rid, problem, targets, arrival
+        self.done = None
+        self.endpoints = self.conv = self.status = None
+
+
+class _Slot:
+    def __init__(self, torch, pb, cap, paths, N, P1):
+        self.cap = cap
+        self.h_tg = torch.zeros((cap, P1, 2), dtype=torch.float64).pin_memory()
+        self.d_tg = torch.zeros((cap, P1, 2), dtype=torch.float64, device="cuda")
+        self.d_diff = torch.zeros((cap, P1, 2), dtype=torch.float64, device="cuda")
+        self.ws = ghc.Workspace(pb, cap, ghc.PREC_FP64, paths=paths)
+        self.h_ep = torch.zeros((cap * paths, N, 2), dtype=torch.float64).pin_memory()
+        self.h_conv = torch.zeros(cap * paths, dtype=torch.uint8).pin_memory()
+        self.h_status = torch.zeros(cap * paths, dtype=torch.uint8).pin_memory()
+        self.event = None
+        self.requests = []
+
+
+class _Problem:
+    def __init__(self, torch, name, cap, slots):
+        self.name = name
+        self.pb = ghc.Problem(name)
+        s, t = self.pb.params()
+        if name == "P3P_TD":
+            (s, _), _ = scenes.p3p_td(1, seed=0)
+        self.start = s
+        self.target = t
+        self.paths = self.pb.paths
+        self.d_start = torch.from_numpy(np.stack([s.real, s.imag], -1).copy()).cuda()
+        sols = self.pb.start_sols()
+        self.d_sols = torch.from_numpy(np.stack([sols.real, sols.imag], -1).copy()).cuda()
+        self.stream = torch.cuda.Stream()
+        self.slots = [_Slot(torch, self.pb, cap, self.paths, self.pb.N, self.pb.P + 1) for _ in range(slots)]
+        self.queue = collections.deque()
+
+
+def bytes_per_hypothesis(pb):
+    P1 = pb.P + 1
+    tables = 16 * (pb.M + 1) * (2 * pb.K + 1) if pb.kind == ghc.KIND_P2C else 0
+    per_path = 16 * pb.N + 3 + 4 * 2 + 8 * 3
+    return 2 * 16 * P1 + tables + pb.paths * (per_path + 16 * pb.N + 2)
+
+
+class Server:
+    def __init__(self, torch, problems=MIX, max_batch=2048, hbm_fraction=0.25, sequential=False):
+        self.torch = torch
+        self.sequential = sequential
+        free, _ = torch.cuda.mem_get_info()
+        slots = 1 if sequential else 2
+        self.problems = {}
+        for name in problems:
+            pb = ghc.Problem(name)
+            budget = hbm_fraction * free / (len(problems) * slots)
+            cap = int(max(1, min(max_batch, budget // bytes_per_hypothesis(pb))))
+            self.problems[name] = _Problem(torch, name, cap, slots)
+        self.fifo = collections.deque()  # sequential mode: global order
+        self.launches = 0
+
+    def submit(self, req):
+        if self.sequential:
+            self.fifo.append(req)
+        else:
+            self.problems[req.problem].queue.append(req)
+
+    def _launch(self, prob, slot, reqs):
+        torch = self.torch
+        n = sum(r.targets.shape[0] for r in reqs)
+        tg = np.concatenate([r.targets for r in reqs])
+        slot.h_tg[:n, :, 0] = torch.from_numpy(tg.real)
+        slot.h_tg[:n, :, 1] = torch.from_numpy(tg.imag)
+        slot.requests = reqs
+        with torch.cuda.stream(prob.stream):
+            slot.d_tg[:n].copy_(slot.h_tg[:n], non_blocking=True)
+            ws = slot.ws
+            ws.n_hyp = n
+            if prob.pb.kind == ghc.KIND_P2C:
+                hx, ht = prob.pb.p2c_device(prob.d_start, slot.d_tg[:n])
+                ghc.track(prob.pb, ws, prob.d_sols, d_coef_hx=hx, d_coef_ht=ht)
+            else:
+                torch.sub(slot.d_tg[:n], prob.d_start[None], out=slot.d_diff[:n])
+                ghc.track(prob.pb, ws, prob.d_sols, d_p_start=prob.d_start, d_p_target=slot.d_tg[:n],
+                          d_p_diff=slot.d_diff[:n])
+            m = n * prob.paths
+            slot.h_ep[:m].copy_(ws.endpoints[:m], non_blocking=True)
+            slot.h_conv[:m].copy_(ws.conv[:m], non_blocking=True)
+            slot.h_status[:m].copy_(ws.status[:m], non_blocking=True)
+            slot.event = torch.cuda.Event()
+            slot.event.record(prob.stream)
+        self.launches += 1
+
+    def _complete(self, prob, slot, now):
+        off = 0
+        for r in slot.requests:
+            m = r.targets.shape[0] * prob.paths
+            e = slot.h_ep[off:off + m].numpy()
+            r.endpoints = e[..., 0] + 1j * e[..., 1]
+            r.conv = slot.h_conv[off:off + m].numpy().copy()
+            r.status = slot.h_status[off:off + m].numpy().copy()
+            r.done = now
+            off += m
+        slot.requests = []
+        slot.event = None
+
+    def step(self, now):
+        """Complete finished batches, then admit queued requests into free slots."""
+        busy = False
+        for prob in self.problems.values():
+            for slot in prob.slots:
+                if slot.event is not None:
+                    if slot.event.query():
+                        self._complete(prob, slot, now)
+                    else:
+                        busy = True
+        if self.sequential:
+            prob = None
+            if self.fifo and not busy:
+                r = self.fifo.popleft()
+                prob = self.problems[r.problem]
+                self._launch(prob, prob.slots[0], [r])
+                busy = True
+            return busy or bool(self.fifo)
+        for prob in self.problems.values():
+            for slot in prob.slots:
+                if slot.event is None and prob.queue:
+                    reqs, n = [], 0
+                    while prob.queue and n + prob.queue[0].targets.shape[0] <= slot.cap:
+                        r = prob.queue.popleft()
+                        reqs.append(r)
+                        n += r.targets.shape[0]
+                    if not reqs:  # a request larger than a slot: split is not done, take it alone
+                        reqs = [prob.queue.popleft()]
+                    self._launch(prob, slot, reqs)
+                    busy = True
+        return busy or any(p.queue for p in self.problems.values())
+
+
+def poisson_requests(lam, n_req, seed=0, problems=MIX, max_hyp=512):
+    """Arrival offsets (s), problem and log-uniform size in [1, max_hyp] of n_req requests."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / lam, size=n_req)
+    t = np.cumsum(gaps) - gaps[0]
+    sizes = np.floor(np.exp(rng.uniform(0, np.log(max_hyp + 1), size=n_req))).astype(int)
+    sizes = np.clip(sizes, 1, max_hyp)
+    which = rng.integers(0, len(problems), size=n_req)
+    return t, [problems[i] for i in which], sizes
+
+
+def run_stream(server, lam, n_req, seed=0):
+    """Feed a Poisson stream in real time; returns (latencies s, hypotheses, wall s)."""
+    t_arr, probs, sizes = poisson_requests(lam, n_req, seed=seed, problems=list(server.problems))
+    reqs = []
+    for i in range(n_req):
+        prob = server.problems[probs[i]]
+        tg = scenes.perturbed_targets(prob.target, int(sizes[i]), seed=seed * 100003 + i) \
+            if probs[i] != "P3P_TD" else scenes.p3p_td(int(sizes[i]), seed=seed * 100003 + i)[0][1]
+        reqs.append(Request(i, probs[i], tg, None))
+    server.torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nxt = 0
+    while True:
+        now = time.perf_counter() - t0
+        while nxt < n_req and t_arr[nxt] <= now:
+            reqs[nxt].arrival = t_arr[nxt]
+            server.submit(reqs[nxt])
+            nxt += 1
+        active = server.step(now)
+        if nxt >= n_req and not active:
+            break
+        if not active and nxt < n_req:
+            time.sleep(min(1e-3, max(0.0, t_arr[nxt] - now)))
+    wall = time.perf_counter() - t0
+    lat = np.array([r.done - r.arrival for r in reqs])
+    return lat, int(sizes.sum()), wall, reqs
+
+
+def bench(args, torch):
+    torch.cuda.set_device(0)
+    lams = [100, 300, 1000, 3000, 10000, 20000]
+    n_req = 60
+    rows = []
+    batched = Server(torch)
+    seq = Server(torch, sequential=True)
+    # warm both (kernel attributes, tables) with a small stream
+    run_stream(batched, 1000, 8, seed=999)
+    run_stream(seq, 1000, 4, seed=998)
+    for lam in lams:
+        lat, hyp, wall, _ = run_stream(batched, lam, n_req, seed=lam)
+        lat_s, hyp_s, wall_s, _ = run_stream(seq, lam, n_req, seed=lam)
+        rows.append({"lambda_req_s": lam, "requests": n_req, "hypotheses": hyp,
+                     "batched": {"throughput": hyp / wall, "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                                 "p99_ms": 1e3 * float(np.percentile(lat, 99)), "wall_s": wall},
+                     "sequential_fp64": {"throughput": hyp_s / wall_s,
+                                         "p50_ms": 1e3 * float(np.percentile(lat_s, 50)),
+                                         "p99_ms": 1e3 * float(np.percentile(lat_s, 99)), "wall_s": wall_s}})
+    best = max(r["batched"]["throughput"] for r in rows)
+    line = {"metric": "served hypothesis-solves/s and p50/p99 request latency vs offered load", "value": best,
+            "unit": "hypotheses/s", "n_gpus": 1, "steps": len(lams), "warmup": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic (seeded)",
+            "config": {"workload": "Poisson request stream, %d requests per load point, 1-512 hypotheses "
+                                   "(log-uniform) of a problem drawn uniformly from %s; continuous batching "
+                                   "on per-problem streams vs one-request-per-launch FP64" % (n_req, MIX)},
+            "capacity_hypotheses_per_launch": {n: p.slots[0].cap for n, p in batched.problems.items()},
+            "sweep": rows}
+    print(json.dumps(line), flush=True)

@@ -1,0 +1,262 @@
+"""Workloads of the scope beyond bench.py's headline (``bench.py --config ...``).
+
+cy       batched: 4096 RANSAC hypotheses of the uncalibrated trifocal problem
+         (12 unknowns, 668 paths; seeded 3-camera scenes, minimal samples with
+         30 % outlier correspondences) -- device P2C + tracker + FP64 polish
+         captured in one CUDA graph and replayed per step.
+p3p_td   P3P by a total-degree homotopy: one instance (latency, p50/p99) and
+         a batch of 65536 instances (throughput), plain FP64.
+mix      uneven mix in one graph launch: P3P_TD 8192, 5-point 4096,
+         generalized 3-view 2048, trifocal 30x30 1024 hypotheses on four
+         streams forked and joined inside one captured graph.
+served   Poisson request stream through serve.Server (continuous batching).
+g3v4_mono  generalized 3-view with start parameters ~ complex N(0,1) and
+         start solutions from the monodromy solver, plain FP64 vs mixed.
+
+Each prints one JSON line with the bench contract's keys.
+"""
+import json
+import os
+import statistics
+import time
+
+import numpy as np
+
+import ghc
+import scenes
+
+UNIT = "hypotheses/s"
+
+
+def _cx(a, torch, dt=None):
+    a = np.asarray(a, dtype=np.complex128)
+    t = torch.from_numpy(np.ascontiguousarray(np.stack([a.real, a.imag], -1)))
+    return t.to(dt or torch.float64).cuda()
+
+
+def _to_cx(t):
+    a = t.double().cpu().numpy()
+    return a[..., 0] + 1j * a[..., 1]
+
+
+def _line(metric, value, args, config, **extra):
+    d = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+         "data": "synthetic (seeded scenes)", "config": config}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+class Batch:
+    """One problem's batch: inputs on the device, a workspace, and the launch."""
+
+    def __init__(self, torch, name, H, seed, precision=ghc.PREC_FP64, polish=0, step=None, start=None, sols=None):
+        self.pb = ghc.Problem(name)
+        s, t = self.pb.params()
+        st, tg, truth = scenes.targets_for(name, H, seed, s, t)
+        if start is not None:
+            st = start
+        self.name, self.H, self.truth, self.targets = name, H, truth, tg
+        self.d_start = _cx(st, torch)
+        self.d_tg = _cx(tg, torch)
+        self.d_diff = _cx(tg - np.asarray(st)[None, :], torch)
+        s0 = self.pb.start_sols() if sols is None else sols
+        self.paths = s0.shape[0]
+        self.d_sols = _cx(s0, torch)
+        self.ws = ghc.Workspace(self.pb, H, precision, paths=self.paths)
+        self.kw = dict(polish_iters=polish, want_resid=polish > 0, t_switch=0.0)
+        if step:
+            self.kw.update(step)
+
+    def launch(self):
+        if self.pb.kind == ghc.KIND_P2C:
+            hx, ht = self.pb.p2c_device(self.d_start, self.d_tg)
+            ghc.track(self.pb, self.ws, self.d_sols, d_coef_hx=hx, d_coef_ht=ht, **self.kw)
+        else:
+            ghc.track(self.pb, self.ws, self.d_sols, d_p_start=self.d_start, d_p_target=self.d_tg,
+                      d_p_diff=self.d_diff, **self.kw)
+
+
+def _time_graph(torch, g, steps, flush):
+    ms = []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return ms
+
+
+def _capture(torch, fn):
+    fn()  # warm-up outside capture: uploads problem tables, sets kernel attributes
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        fn()
+    torch.cuda.synchronize()
+    return g
+
+
+def config_cy(args, torch):
+    H = args.hyp if args.hyp != 1024 else 4096
+    b = Batch(torch, "uncalibrated_trifocal_rel_pos_CY", H, 1000 + args.seed, polish=2)
+    _, _, inlier = scenes.uncalibrated_trifocal_rel_pos_CY(H, seed=1000 + args.seed)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    g = _capture(torch, b.launch)
+    for _ in range(args.warmup):
+        g.replay()
+    torch.cuda.synchronize()
+    ms = _time_graph(torch, g, args.steps, flush)
+    ep = _to_cx(b.ws.endpoints).reshape(H, b.paths, -1)
+    conv = b.ws.conv.cpu().numpy().reshape(H, b.paths) == 1
+    found = 0
+    for h in np.nonzero(inlier)[0]:
+        E = ep[h][conv[h]]
+        best = 9.0
+        for s2 in (1, -1):
+            for s3 in (1, -1):
+                gt = b.truth[h].copy()
+                gt[4:8] *= s2
+                gt[8:12] *= s3
+                if E.size:
+                    best = min(best, (np.abs(E - gt).max(axis=1) / np.abs(gt).max()).min())
+        found += best < 1e-2
+    steps = b.ws.steps.cpu().numpy()
+    total = sum(ms)
+    _line("hypothesis-solves/s (batched, one graph replay per step)", H * len(ms) / (total * 1e-3), args,
+          {"workload": "uncalibrated_trifocal_rel_pos_CY: %d RANSAC hypotheses x 668 paths (%d paths) per step, "
+                       "30%% outlier correspondences, FP64, reference step control, FP64 polish, one CUDA graph"
+                       % (H, H * b.paths), "hypotheses_per_step": H, "l2": "flushed before each step"},
+          ms_per_step=total / len(ms), p50_ms=float(np.percentile(ms, 50)), p99_ms=float(np.percentile(ms, 99)),
+          paths={"per_step": H * b.paths, "converged_frac": float(conv.mean()), "mean_steps": float(steps.mean()),
+                 "max_steps": int(steps.max())},
+          inlier_hypotheses=int(inlier.sum()), inlier_ground_truth_found=found / max(1, int(inlier.sum())),
+          gpu_launches=3 * args.steps)
+
+
+def config_p3p_td(args, torch):
+    single = Batch(torch, "P3P_TD", 1, 7 + args.seed, polish=2)
+    lat = []
+    for i in range(args.warmup + max(args.steps, 50)):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        single.launch()
+        e1.record()
+        e1.synchronize()
+        if i >= args.warmup:
+            lat.append(e0.elapsed_time(e1))
+    E = _to_cx(single.ws.endpoints)
+    gt_ok = bool(np.abs(E - single.truth[0]).max(axis=1).min() < 1e-9)
+    H = 65536
+    batch = Batch(torch, "P3P_TD", H, 8 + args.seed, polish=2)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    g = _capture(torch, batch.launch)
+    for _ in range(args.warmup):
+        g.replay()
+    ms = _time_graph(torch, g, args.steps, flush)
+    E = _to_cx(batch.ws.endpoints).reshape(H, 8, 3)
+    hit = np.mean([np.abs(E[h] - batch.truth[h]).max(axis=1).min() < 1e-9 for h in range(0, H, 64)])
+    _line("hypothesis-solves/s (P3P total degree)", H * len(ms) / (sum(ms) * 1e-3), args,
+          {"workload": "P3P_TD: 3 depths, 8 total-degree paths, seeded unit-modulus gamma; 1 instance (latency) "
+                       "and %d instances per step (throughput); FP64 with polish" % H},
+          ms_per_step=sum(ms) / len(ms), single_instance={"p50_ms": float(np.percentile(lat, 50)),
+                                                          "p99_ms": float(np.percentile(lat, 99)),
+                                                          "ground_truth_found": gt_ok},
+          ground_truth_found_frac=float(hit), gpu_launches=3 * args.steps)
+
+
+MIX = [("P3P_TD", 8192), ("5pt_rel_pos_alg_form_quat", 4096), ("generalized_3views_4pts", 2048),
+       ("trifocal_2op1p_30x30", 1024)]
+
+
+def config_mix(args, torch):
+    batches = [Batch(torch, n, h, 50 + i + args.seed) for i, (n, h) in enumerate(MIX)]
+    streams = [torch.cuda.Stream() for _ in batches]
+
+    def fork_join():
+        main = torch.cuda.current_stream()
+        ev = torch.cuda.Event()
+        ev.record(main)
+        for b, st in zip(batches, streams):
+            with torch.cuda.stream(st):
+                st.wait_event(ev)
+                b.launch()
+        for st in streams:
+            main.wait_stream(st)
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    g = _capture(torch, fork_join)
+    for _ in range(args.warmup):
+        g.replay()
+    ms = _time_graph(torch, g, args.steps, flush)
+    # each problem alone, for the overlap benefit
+    alone = {}
+    for b in batches:
+        gb = _capture(torch, b.launch)
+        alone[b.name] = statistics.median(_time_graph(torch, gb, 2, flush))
+    total_h = sum(h for _, h in MIX)
+    _line("hypothesis-solves/s (uneven mix, one graph launch)", total_h * len(ms) / (sum(ms) * 1e-3), args,
+          {"workload": "uneven mix in one CUDA graph: " + ", ".join("%s %d hyp" % m for m in MIX) +
+                       "; four streams forked and joined inside the graph; FP64, reference step control"},
+          ms_per_step=sum(ms) / len(ms), alone_ms=alone, sum_alone_ms=sum(alone.values()),
+          per_problem={b.name: {"hypotheses": b.H, "paths": b.H * b.paths,
+                                "converged_frac": float(b.ws.conv.float().mean())} for b in batches},
+          gpu_launches=8 * args.steps)
+
+
+def config_g3v4_mono(args, torch):
+    import monodromy
+    pb = ghc.Problem("generalized_3views_4pts")
+    t0 = time.time()
+    q, Sq, S = monodromy.start_system(pb, seed=args.seed)
+    mono_s = time.time() - t0
+    H = min(args.hyp, 512)
+    out = {}
+    runs = {}
+    step = dict(step=dict(corr_tol2=1e-12, first_tol2=1e-2, dt_max=0.05), max_corr=3, max_steps=2000)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    for name, prec in (("fp64", ghc.PREC_FP64), ("mixed", ghc.PREC_MIXED)):
+        b = Batch(torch, "generalized_3views_4pts", H, 77 + args.seed, precision=prec, polish=3, step=step,
+                  start=q, sols=Sq)
+        g = _capture(torch, b.launch)
+        ms = _time_graph(torch, g, max(1, args.steps // 2), flush)
+        runs[name] = (_to_cx(b.ws.endpoints).reshape(H, b.paths, -1), b.ws.conv.cpu().numpy().reshape(H, -1) == 1,
+                      b.truth)
+        out[name] = {"value": H / (statistics.median(ms) * 1e-3), "unit": UNIT, "ms": statistics.median(ms)}
+    e64, c64, truth = runs["fp64"]
+    emx, cmx, _ = runs["mixed"]
+    real = 0
+    found = 0
+    gt_hits = 0
+    for h in range(H):
+        r = e64[h][c64[h] & (np.abs(e64[h].imag).max(axis=1) <= 1e-8)]
+        m = emx[h][cmx[h]]
+        for e in r:
+            real += 1
+            d = np.abs(m - e).max(axis=1) / max(1.0, np.abs(e).max())
+            found += bool(d.size and d.min() <= 1e-8)
+        E = e64[h][c64[h]]
+        gt_hits += bool(E.size and (np.abs(E - truth[h]).max(axis=1) / np.abs(truth[h]).max()).min() < 1e-2)
+    _line("hypothesis-solves/s at real-sol recall, mixed vs plain FP64 (own start system)", out["mixed"]["value"],
+          args, {"workload": "generalized_3views_4pts: start params ~ complex N(0,1) (seed %d), %d start solutions "
+                             "from the monodromy solver, %d seeded scenes (0.5 px noise) per step, path-jump-free "
+                             "step control, FP64 polish" % (args.seed, len(Sq), H)},
+          modes=out, recall_mixed_vs_fp64=found / max(1, real), real_solutions_fp64=real,
+          ground_truth_found_frac=gt_hits / H, monodromy={"solutions": len(S), "seconds": mono_s})
+
+
+def config_served(args, torch):
+    import serve
+    serve.bench(args, torch)
+
+
+def run(args):
+    import torch
+    torch.cuda.set_device(0)
+    {"cy": config_cy, "p3p_td": config_p3p_td, "mix": config_mix, "served": config_served,
+     "g3v4_mono": config_g3v4_mono}[args.config](args, torch)

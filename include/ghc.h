@@ -135,6 +135,8 @@ typedef struct {
   double* d_resid;            /* [n_items] |H(x,1)| after polish, -1 if not converged (optional) */
   /* scratch */
   int32_t* d_counter;         /* one int of device memory (work-stealing counter) */
+  /* start solutions per hypothesis in d_start_sols; <= 0: the problem's Num_Of_Tracks */
+  int32_t paths;
 } ghc_track_args;
 
 int ghc_track(const ghc_problem* pb, const ghc_track_args* args, void* stream);

@@ -1,0 +1,56 @@
+"""Serving loop (needs a B200): every request's result is the same alone and in the mix.
+
+Requests of two problems arrive as a Poisson stream and are packed into
+shared launches by serve.Server; each request is then tracked alone with
+ghc.track on the same targets.  Per-hypothesis arithmetic does not depend on
+the batch, so endpoints and flags must be identical (the same bit-for-bit bar
+as the other FP64 parity tests).  The monodromy solver is checked here too.
+"""
+import numpy as np
+import pytest
+
+import ghc
+import serve
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def cx_t(a):
+    a = np.asarray(a, dtype=np.complex128)
+    return torch.from_numpy(np.ascontiguousarray(np.stack([a.real, a.imag], -1))).cuda()
+
+
+def test_requests_same_alone_and_in_the_mix():
+    server = serve.Server(torch, problems=["P3P_TD", "generalized_3views_4pts"], max_batch=256)
+    lat, hyp, wall, reqs = serve.run_stream(server, lam=2000, n_req=12, seed=4)
+    assert all(r.done is not None for r in reqs)
+    assert server.launches < len(reqs)  # requests did share launches
+    for r in reqs:
+        prob = server.problems[r.problem]
+        n = r.targets.shape[0]
+        ws = ghc.Workspace(prob.pb, n, ghc.PREC_FP64)
+        hx, ht = prob.pb.p2c_device(prob.d_start, cx_t(r.targets))
+        ghc.track(prob.pb, ws, prob.d_sols, d_coef_hx=hx, d_coef_ht=ht)
+        torch.cuda.synchronize()
+        e = ws.endpoints.cpu().numpy()
+        e = e[..., 0] + 1j * e[..., 1]
+        assert np.array_equal(ws.conv.cpu().numpy(), r.conv)
+        fin = np.isfinite(e)
+        assert np.array_equal(e[fin], r.endpoints[fin])
+
+
+def test_sequential_baseline_matches_batched():
+    b = serve.Server(torch, problems=["P3P_TD"], max_batch=64)
+    s = serve.Server(torch, problems=["P3P_TD"], sequential=True, max_batch=64)
+    _, _, _, rb = serve.run_stream(b, lam=5000, n_req=6, seed=8)
+    _, _, _, rs = serve.run_stream(s, lam=5000, n_req=6, seed=8)
+    for x, y in zip(rb, rs):
+        assert np.array_equal(x.endpoints, y.endpoints)
+
+
+def test_monodromy_finds_all_p3p_solutions():
+    import monodromy
+    pb = ghc.Problem("P3P")
+    q, Sq, S = monodromy.start_system(pb, seed=3)
+    assert len(S) == 8 and len(Sq) == 8

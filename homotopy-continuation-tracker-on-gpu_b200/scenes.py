@@ -221,13 +221,15 @@ def perturbed_targets(target, n_hyp, seed=0, scale=0.05):
     return out
 
 
-def targets_for(name, n_hyp, seed, start, shipped_target):
-    """(start params [P+1], targets [H, P+1], truth or None) for a problem's batch."""
+def targets_for(name, n_hyp, seed, start, shipped_target, **scene):
+    """(start params [P+1], targets [H, P+1], truth or None) for a problem's batch.
+
+    ``scene`` is passed to the problem's scene generator (e.g. noise_px)."""
     if name == "generalized_3views_4pts":
-        tg, truth = generalized_3views_4pts(n_hyp, seed=seed)
+        tg, truth = generalized_3views_4pts(n_hyp, seed=seed, **scene)
         return start, tg, truth
     if name == "uncalibrated_trifocal_rel_pos_CY":
-        tg, truth, _ = uncalibrated_trifocal_rel_pos_CY(n_hyp, seed=seed)
+        tg, truth, _ = uncalibrated_trifocal_rel_pos_CY(n_hyp, seed=seed, **scene)
         return start, tg, truth
     if name == "P3P_TD":
         (st, tg), truth = p3p_td(n_hyp, seed=seed)

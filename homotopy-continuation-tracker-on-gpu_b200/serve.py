@@ -81,7 +81,7 @@ def bytes_per_hypothesis(pb):
 
 
 class Server:
-    def __init__(self, torch, problems=MIX, max_batch=2048, hbm_fraction=0.25, sequential=False):
+    def __init__(self, torch, problems=MIX, max_batch=2048, hbm_fraction=0.25, sequential=False, max_request=512):
         self.torch = torch
         self.sequential = sequential
         free, _ = torch.cuda.mem_get_info()
@@ -90,12 +90,18 @@ class Server:
         for name in problems:
             pb = ghc.Problem(name)
             budget = hbm_fraction * free / (len(problems) * slots)
-            cap = int(max(1, min(max_batch, budget // bytes_per_hypothesis(pb))))
+            cap = int(min(max(max_batch, max_request), budget // bytes_per_hypothesis(pb)))
+            if cap < max_request:
+                raise MemoryError("%s: %d hypotheses per slot fit in the memory budget, requests may have %d"
+                                  % (name, cap, max_request))
             self.problems[name] = _Problem(torch, name, cap, slots)
         self.fifo = collections.deque()  # sequential mode: global order
         self.launches = 0
 
     def submit(self, req):
+        cap = self.problems[req.problem].slots[0].cap
+        if req.targets.shape[0] > cap:
+            raise ValueError("request of %d hypotheses exceeds the %d of a launch slot" % (req.targets.shape[0], cap))
         if self.sequential:
             self.fifo.append(req)
         else:
@@ -166,8 +172,6 @@ class Server:
                         r = prob.queue.popleft()
                         reqs.append(r)
                         n += r.targets.shape[0]
-                    if not reqs:  # a request larger than a slot: split is not done, take it alone
-                        reqs = [prob.queue.popleft()]
                     self._launch(prob, slot, reqs)
                     busy = True
         return busy or any(p.queue for p in self.problems.values())

@@ -50,10 +50,11 @@ def _line(metric, value, args, config, **extra):
 class Batch:
     """One problem's batch: inputs on the device, a workspace, and the launch."""
 
-    def __init__(self, torch, name, H, seed, precision=ghc.PREC_FP64, polish=0, step=None, start=None, sols=None):
+    def __init__(self, torch, name, H, seed, precision=ghc.PREC_FP64, polish=0, step=None, start=None, sols=None,
+                 scene=None):
         self.pb = ghc.Problem(name)
         s, t = self.pb.params()
-        st, tg, truth = scenes.targets_for(name, H, seed, s, t)
+        st, tg, truth = scenes.targets_for(name, H, seed, s, t, **(scene or {}))
         if start is not None:
             st = start
         self.name, self.H, self.truth, self.targets = name, H, truth, tg
@@ -103,8 +104,12 @@ def _capture(torch, fn):
 
 def config_cy(args, torch):
     H = args.hyp if args.hyp != 1024 else 4096
-    b = Batch(torch, "uncalibrated_trifocal_rel_pos_CY", H, 1000 + args.seed, polish=2)
-    _, _, inlier = scenes.uncalibrated_trifocal_rel_pos_CY(H, seed=1000 + args.seed)
+    # Inlier correspondences are exact (no pixel noise), so an all-inlier hypothesis has the
+    # scene's unknowns as an exact solution and the known answer can be checked at 1e-6.  With
+    # 0.5 px noise this minimal problem is so ill-conditioned (focal length from 4 points) that
+    # the nearest solution moves 10-40 % away from the noise-free scene.
+    b = Batch(torch, "uncalibrated_trifocal_rel_pos_CY", H, 1000 + args.seed, polish=2, scene={"noise_px": 0.0})
+    _, _, inlier = scenes.uncalibrated_trifocal_rel_pos_CY(H, seed=1000 + args.seed, noise_px=0.0)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     g = _capture(torch, b.launch)
     for _ in range(args.warmup):
@@ -124,12 +129,12 @@ def config_cy(args, torch):
                 gt[8:12] *= s3
                 if E.size:
                     best = min(best, (np.abs(E - gt).max(axis=1) / np.abs(gt).max()).min())
-        found += best < 1e-2
+        found += best < 1e-6
     steps = b.ws.steps.cpu().numpy()
     total = sum(ms)
     _line("hypothesis-solves/s (batched, one graph replay per step)", H * len(ms) / (total * 1e-3), args,
           {"workload": "uncalibrated_trifocal_rel_pos_CY: %d RANSAC hypotheses x 668 paths (%d paths) per step, "
-                       "30%% outlier correspondences, FP64, reference step control, FP64 polish, one CUDA graph"
+                       "30%% outlier correspondences (inliers exact), FP64, reference step control, FP64 polish, one CUDA graph"
                        % (H, H * b.paths), "hypotheses_per_step": H, "l2": "flushed before each step"},
           ms_per_step=total / len(ms), p50_ms=float(np.percentile(ms, 50)), p99_ms=float(np.percentile(ms, 99)),
           paths={"per_step": H * b.paths, "converged_frac": float(conv.mean()), "mean_steps": float(steps.mean()),

@@ -22,7 +22,7 @@ def cx_t(a):
 
 
 def test_requests_same_alone_and_in_the_mix():
-    server = serve.Server(torch, problems=["P3P_TD", "generalized_3views_4pts"], max_batch=256)
+    server = serve.Server(torch, problems=["P3P_TD", "generalized_3views_4pts"], max_batch=512)
     lat, hyp, wall, reqs = serve.run_stream(server, lam=2000, n_req=12, seed=4)
     assert all(r.done is not None for r in reqs)
     assert server.launches < len(reqs)  # requests did share launches
@@ -41,8 +41,8 @@ def test_requests_same_alone_and_in_the_mix():
 
 
 def test_sequential_baseline_matches_batched():
-    b = serve.Server(torch, problems=["P3P_TD"], max_batch=64)
-    s = serve.Server(torch, problems=["P3P_TD"], sequential=True, max_batch=64)
+    b = serve.Server(torch, problems=["P3P_TD"], max_batch=512)
+    s = serve.Server(torch, problems=["P3P_TD"], sequential=True, max_batch=512)
     _, _, _, rb = serve.run_stream(b, lam=5000, n_req=6, seed=8)
     _, _, _, rs = serve.run_stream(s, lam=5000, n_req=6, seed=8)
     for x, y in zip(rb, rs):

@@ -47,7 +47,11 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--quick", action="store_true", help="skip the secondary modes and the CPU baseline")
-    ap.add_argument("--config", default="g3v4", choices=["g3v4", "cy", "p3p_td", "mix", "served", "g3v4_mono"],
+    ap.add_argument("--problem", default="trifocal_2op1p_30x30", help="problem folder for --config problem")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "mixed"], help="for --config problem")
+    ap.add_argument("--step", default="reference", choices=["reference", "robust"], help="for --config problem")
+    ap.add_argument("--config", default="g3v4", choices=["g3v4", "cy", "p3p_td", "mix", "served", "g3v4_mono",
+                                                          "problem"],
                     help="g3v4: the headline (default); the others are the remaining workloads of the scope")
     return ap.parse_args()
 

@@ -72,6 +72,7 @@ TrackParams base_params(const Problem& pb) {
   p.hx_off = pb.dev.hx_off;
   p.ht_terms = pb.dev.ht_terms;
   p.ht_off = pb.dev.ht_off;
+  p.flat_eval = flat_eval_pays(pb.hx_off.data(), pb.N);
   p.t_switch = 2.0;
   // the reference's step control (kernel_HC_Solver_P3P.cu:214): no contraction test, no step cap
   p.corr_tol2 = 1e-6;
@@ -90,6 +91,7 @@ PolishParams polish_params(const TrackParams& t, double* endpoints, const uint8_
   q.K = t.K;
   q.n_hx_terms = t.n_hx_terms;
   q.n_ht_terms = t.n_ht_terms;
+  q.flat_eval = t.flat_eval;
   q.hx_terms = t.hx_terms;
   q.hx_off = t.hx_off;
   q.ht_terms = t.ht_terms;
@@ -155,6 +157,7 @@ int dropin_tables(Problem& pb, const int* d_hx, const int* d_ht, TrackParams& p,
   p.ht_off = (const uint16_t*)d;
   p.n_hx_terms = (int)hxt.size();
   p.n_ht_terms = (int)htt.size();
+  p.flat_eval = flat_eval_pays(hxo.data(), pb.N);
   return GHC_OK;
 }
 

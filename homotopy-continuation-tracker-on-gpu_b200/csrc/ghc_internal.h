@@ -24,20 +24,45 @@ enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1, PREC_MIXED = 2 };
 enum Status : int { ST_CONVERGED = 0, ST_DIVERGED = 1, ST_STEP_CAP = 2 };
 
 constexpr int kMaxN = 32;
-constexpr int kMaxVarsPerTerm = 8;
+constexpr int kMaxVarsPerTerm = 7;
 
 // term word layout
 //   bits  0.. 7  integer scale (int8)
 //   bits  8..10  number of variable factors nv (slot N, the constant 1, dropped)
 //   bits 11..20  P2C: coefficient index k (0..1023)
 //   bits 11..16  PH : parameter index a ; bits 17..22 PH: parameter index b
-//   bits 24..63  variable indices, 5 bits each, table order
+//   bits 24..58  variable indices, 5 bits each, table order
+//   bits 59..63  H_x terms: the Jacobian column of the term (its row is implied by the CSR row)
 GHC_HD inline int term_scale(uint64_t w) { return (int)(int8_t)(w & 0xffu); }
 GHC_HD inline int term_nv(uint64_t w) { return (int)((w >> 8) & 7u); }
 GHC_HD inline int term_coef(uint64_t w) { return (int)((w >> 11) & 0x3ffu); }
 GHC_HD inline int term_pa(uint64_t w) { return (int)((w >> 11) & 0x3fu); }
 GHC_HD inline int term_pb(uint64_t w) { return (int)((w >> 17) & 0x3fu); }
 GHC_HD inline int term_var(uint64_t w, int q) { return (int)((w >> (24 + 5 * q)) & 31u); }
+GHC_HD inline int term_col(uint64_t w) { return (int)(w >> 59); }
+
+// Whether the tracker should walk each H_x row as one term list (staging the
+// entries in shared memory) rather than entry by entry.  Entry by entry, a
+// sub-warp runs, for every column, as many iterations as the row with the most
+// terms in that column; row-wise it runs as many as the longest row.  Above
+// 16 unknowns the kernels always walk rows (entry-wise code would be unrolled
+// N times).  hx_off: CSR offsets [N*N+1] of the compiled H_x terms.
+inline int flat_eval_pays(const uint16_t* hx_off, int N) {
+  int longest = 0, per_entry = 0;
+  for (int r = 0; r < N; ++r) {
+    const int len = hx_off[r * N + N] - hx_off[r * N];
+    if (len > longest) longest = len;
+  }
+  for (int i = 0; i < N; ++i) {
+    int m = 0;
+    for (int r = 0; r < N; ++r) {
+      const int c = hx_off[r * N + i + 1] - hx_off[r * N + i];
+      if (c > m) m = c;
+    }
+    per_entry += m;
+  }
+  return 4 * per_entry > 5 * longest ? 1 : 0;
+}
 
 // Everything the tracker kernel needs, by value.
 struct TrackParams {
@@ -45,6 +70,7 @@ struct TrackParams {
   int kind, N, P, M, K;
   int max_steps, max_corr, incr;
   int n_hx_terms, n_ht_terms;
+  int flat_eval;              // flat_eval_pays() of the tables
   const uint64_t* hx_terms;   // device
   const uint16_t* hx_off;     // device [N*N+1]
   const uint64_t* ht_terms;   // device
@@ -88,6 +114,7 @@ struct TrackParams {
 struct PolishParams {
   int kind, N, P, M, K;
   int n_hx_terms, n_ht_terms;
+  int flat_eval;
   const uint64_t* hx_terms;
   const uint16_t* hx_off;
   const uint64_t* ht_terms;

@@ -180,7 +180,7 @@ int compile_tables(const std::vector<int32_t>& hx, const std::vector<int32_t>& h
         uint64_t w;
         const int rc = encode(e, Px, w);
         if (rc) return rc;
-        hx_terms.push_back(w);
+        hx_terms.push_back(w | (uint64_t)i << 59);
       }
     }
   }

@@ -156,28 +156,64 @@ __device__ __forceinline__ void coef_eval_ph(const double* __restrict__ ps, cons
   }
 }
 
+// term value p (coefficient, or product of two homotopy parameters, times the integer scale)
+template <typename R, int KIND>
+__device__ __forceinline__ cx<R> term_coef_value(uint64_t w, const cx<R>* ca) {
+  if (KIND == KIND_P2C) return c_scale((R)term_scale(w), ca[term_coef(w)]);
+  const cx<R> p = c_scale((R)term_scale(w), ca[term_pa(w)]);
+  return c_mul(p, ca[term_pb(w)]);
+}
+
 // Row r of H_x into A, and b = H (which = 0) or -H_t (which = 1).
-template <typename R, int N, int KIND>
+//
+// Flat (always above 16 unknowns, else when the problem's flat_eval is set):
+// the row's terms are walked as one list (CSR row r, column in the term word),
+// so a sub-warp spends max_r(terms of row r) iterations instead of
+// sum_i max_r(terms of entry (r, i)).  Each entry's sum is staged in the
+// sub-warp's scratch row scr[i][r] (16-byte slots) and read back into
+// registers; entries without terms are never written and stay zero from the
+// kernel's start.  Entry-wise: one loop per column, straight into registers.
+// Either way every entry is summed in table order, as in the oracle.
+template <int N>
+constexpr bool kFlatAlways = N > 16;
+
+template <typename R, int N, int W, int KIND>
 __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, const cx<R>* cb, const cx<R>* xs, int r,
-                                         bool live, cx<R> (&A)[N], cx<R>& b, int which) {
+                                         bool live, cx<R> (&A)[N], cx<R>& b, int which, bool flat,
+                                         unsigned char* scr) {
+  auto slot = [&](int i) -> cx<R>* { return reinterpret_cast<cx<R>*>(scr + 16 * (size_t)(i * W + r)); };
+  if (!kFlatAlways<N> && !flat) {
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    cx<R> acc = mk(R(0), R(0));
+    for (int i = 0; i < N; ++i) {
+      cx<R> acc = mk(R(0), R(0));
+      if (live) {
+        const int j0 = tb.hx_off[r * N + i], j1 = tb.hx_off[r * N + i + 1];
+        for (int j = j0; j < j1; ++j) {
+          const uint64_t w = tb.hx_terms[j];
+          acc = acc_term(acc, term_coef_value<R, KIND>(w, ca), w, xs);
+        }
+      }
+      A[i] = acc;
+    }
+  } else {
     if (live) {
-      const int j0 = tb.hx_off[r * N + i], j1 = tb.hx_off[r * N + i + 1];
+      const int j0 = tb.hx_off[r * N], j1 = tb.hx_off[r * N + N];
+      int cur = -1;
+      cx<R> acc = mk(R(0), R(0));
       for (int j = j0; j < j1; ++j) {
         const uint64_t w = tb.hx_terms[j];
-        cx<R> p;
-        if (KIND == KIND_P2C) {
-          p = c_scale((R)term_scale(w), ca[term_coef(w)]);
-        } else {
-          p = c_scale((R)term_scale(w), ca[term_pa(w)]);
-          p = c_mul(p, ca[term_pb(w)]);
+        const int i = term_col(w);
+        if (i != cur) {
+          if (cur >= 0) *slot(cur) = acc;
+          acc = mk(R(0), R(0));
+          cur = i;
         }
-        acc = acc_term(acc, p, w, xs);
+        acc = acc_term(acc, term_coef_value<R, KIND>(w, ca), w, xs);
       }
+      if (cur >= 0) *slot(cur) = acc;
     }
-    A[i] = acc;
+#pragma unroll
+    for (int i = 0; i < N; ++i) A[i] = live ? *slot(i) : mk(R(0), R(0));
   }
   cx<R> h = mk(R(0), R(0));
   if (live) {
@@ -214,30 +250,58 @@ __device__ __forceinline__ unsigned pivot_key(R v, int pos, int i) {
   return ((mag_bits(v) >> 5) << 5) | (unsigned)(31 - pos);
 }
 
+// compile-time loop: f(integral_constant<int, I>) for I in [B, E)
+template <int B, int E, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (B < E) {
+    f(std::integral_constant<int, B>{});
+    static_for<B + 1, E>(f);
+  }
+}
+
 // Partial-pivot LU + back substitution, one row per lane, rows in registers.
 // The pivot is found by an integer max butterfly over the sub-warp.  A
 // zero pivot skips that column's elimination and leaves a non-finite
 // solution, as in the reference.  Solution lands in sol[0..N); sx holds
 // N+1 entries (pivot row + its right-hand side).
+//
+// Two code shapes with the same operations in the same order:
+//   LU_UNROLLED  every column unrolled at compile time (template recursion, so
+//                the row stays in registers at any N; code grows as N^2),
+//   LU_ROLLED    a rolled column loop whose row update runs over all N entries
+//                predicated on j > i (N^2 instead of N^2/2 issue slots, code
+//                linear in N).
+// pragma unroll alone gives up above N = 16 and moves the row to local memory.
+constexpr int LU_UNROLLED = 0, LU_ROLLED = 1;
+#ifndef GHC_LU_LARGE
+#define GHC_LU_LARGE LU_UNROLLED
+#endif
+template <int N>
+constexpr int kLuForm = N <= 16 ? LU_UNROLLED : GHC_LU_LARGE;
+
+template <typename R, int W>
+__device__ __forceinline__ int pivot_search(cx<R> a, bool live, int pos, int i) {
+  unsigned best = live ? pivot_key(fabs(a.re) + fabs(a.im), pos, i) : 0u;
+#pragma unroll
+  for (int off = W / 2; off > 0; off >>= 1) best = max(best, __shfl_xor_sync(kFull, best, off, W));
+  return 31 - (int)(best & 31u);
+}
+
 template <typename R, int N, int W>
-__device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
+__device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
   const bool live = l < N;
   int pos = l;
   cx<R> myrcp = mk(R(0), R(0));
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-    unsigned best = live ? pivot_key(fabs(A[i].re) + fabs(A[i].im), pos, i) : 0u;
-#pragma unroll
-    for (int off = W / 2; off > 0; off >>= 1) best = max(best, __shfl_xor_sync(kFull, best, off, W));
-    const int bp = 31 - (int)(best & 31u);
+  static_for<0, N>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const int bp = pivot_search<R, W>(A[i], live, pos, i);
     const bool is_piv = live && (pos == bp);
     if (live) {
       if (pos == bp) pos = i;
       else if (pos == i) pos = bp;
     }
     if (is_piv) {
-#pragma unroll
-      for (int j = i; j < N; ++j) sx[j] = A[j];
+      static_for<i, N>([&](auto jc) { sx[decltype(jc)::value] = A[decltype(jc)::value]; });
       sx[N] = b;
     }
     __syncwarp(kFull);
@@ -247,20 +311,83 @@ __device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* s
     if (is_piv) myrcp = rc;
     if (live && pos > i && !zero) {
       A[i] = c_mul(A[i], rc);
-#pragma unroll
-      for (int j = i + 1; j < N; ++j) A[j] = c_fnma(A[i], sx[j], A[j]);
+      static_for<i + 1, N>([&](auto jc) {
+        constexpr int j = decltype(jc)::value;
+        A[j] = c_fnma(A[i], sx[j], A[j]);
+      });
       b = c_fnma(A[i], sx[N], b);
     }
     __syncwarp(kFull);
-  }
-#pragma unroll
-  for (int i = N - 1; i >= 0; --i) {
+  });
+  static_for<0, N>([&](auto ic) {
+    constexpr int i = N - 1 - decltype(ic)::value;
     if (live && pos == i) sol[i] = c_mul(b, myrcp);
     __syncwarp(kFull);
     const cx<R> xi = sol[i];
     if (live && pos < i) b = c_fnma(A[i], xi, b);
+  });
+  __syncwarp(kFull);
+}
+
+template <typename R, int N>
+__device__ __forceinline__ cx<R> pick(const cx<R> (&A)[N], int i) {
+  cx<R> a = A[0];
+#pragma unroll
+  for (int j = 1; j < N; ++j)
+    if (j == i) a = A[j];
+  return a;
+}
+
+template <typename R, int N, int W>
+__device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
+  const bool live = l < N;
+  int pos = l;
+  cx<R> myrcp = mk(R(0), R(0));
+#pragma unroll 1
+  for (int i = 0; i < N; ++i) {
+    cx<R> ai = pick(A, i);
+    const int bp = pivot_search<R, W>(ai, live, pos, i);
+    const bool is_piv = live && (pos == bp);
+    if (live) {
+      if (pos == bp) pos = i;
+      else if (pos == i) pos = bp;
+    }
+    if (is_piv) {
+#pragma unroll
+      for (int j = 0; j < N; ++j)
+        if (j >= i) sx[j] = A[j];
+      sx[N] = b;
+    }
+    __syncwarp(kFull);
+    const cx<R> p_i = sx[i];
+    const bool zero = (fabs(p_i.re) + fabs(p_i.im) == R(0));
+    const cx<R> rc = c_rcp(zero ? mk(R(0), R(0)) : p_i);
+    if (is_piv) myrcp = rc;
+    if (live && pos > i && !zero) {
+      ai = c_mul(ai, rc);
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        if (j == i) A[j] = ai;
+        if (j > i) A[j] = c_fnma(ai, sx[j], A[j]);
+      }
+      b = c_fnma(ai, sx[N], b);
+    }
+    __syncwarp(kFull);
+  }
+#pragma unroll 1
+  for (int i = N - 1; i >= 0; --i) {
+    if (live && pos == i) sol[i] = c_mul(b, myrcp);
+    __syncwarp(kFull);
+    const cx<R> xi = sol[i];
+    if (live && pos < i) b = c_fnma(pick(A, i), xi, b);
   }
   __syncwarp(kFull);
+}
+
+template <typename R, int N, int W>
+__device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
+  if constexpr (kLuForm<N> == LU_ROLLED) lu_solve_rolled<R, N, W>(A, b, l, sx, sol);
+  else lu_solve_unrolled<R, N, W>(A, b, l, sx, sol);
 }
 
 // xor-butterfly sum over the first NP lanes of the sub-warp (order = oracle tree_sum)
@@ -280,6 +407,7 @@ struct SubMem {
   unsigned char* xs;     // track in stage precision [N+1]
   unsigned char* sx;     // pivot row + rhs [N+1]
   unsigned char* sol;    // solution [N]
+  unsigned char* scr;    // H_x row scratch [N][W] 16-byte slots (both precisions), null unless flat
 };
 
 template <typename R>
@@ -292,7 +420,8 @@ template <typename R, int N, int W, int KIND>
 __device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, int l, int which) {
   cx<R> A[N];
   cx<R> b;
-  eval_row<R, N, KIND>(tb, view<R>(sm.coefA), view<R>(sm.coefB), view<R>(sm.xs), l, l < N, A, b, which);
+  eval_row<R, N, W, KIND>(tb, view<R>(sm.coefA), view<R>(sm.coefB), view<R>(sm.xs), l, l < N, A, b, which,
+                          sm.scr != nullptr, sm.scr);
   lu_solve<R, N, W>(A, b, l, view<R>(sm.sx), view<R>(sm.sol));
   const cx<R> k = (l < N) ? view<R>(sm.sol)[l] : mk(R(0), R(0));
   return k;
@@ -321,8 +450,17 @@ __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t
 __host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
   return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(N * N + 1 + N + 1));
 }
-__host__ __device__ inline size_t sub_bytes(int N, int Mc, bool mixed = false, int W = 0) {
-  return align16(16 * (size_t)(2 * Mc * (mixed ? 2 : 1) + (N + 1) + (N + 1) + N + 2 * W));
+// per sub-warp: coefficient buffers (two sets when mixed), track, pivot row, solution,
+// two lane-state slots per lane, the H_x scratch row [N][W] when the evaluation is flat
+__host__ __device__ inline size_t sub_bytes(int N, int Mc, bool mixed, int W, bool flat) {
+  return align16(16 * (size_t)(2 * Mc * (mixed ? 2 : 1) + (N + 1) + (N + 1) + N + 2 * W + (flat ? N * W : 0)));
+}
+
+// zero this lane's slots of the scratch row (lane l owns slots i*W + l)
+template <int N, int W>
+__device__ __forceinline__ void zero_scratch(unsigned char* scr, int l) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) *reinterpret_cast<double2*>(scr + 16 * (size_t)(i * W + l)) = make_double2(0.0, 0.0);
 }
 
 // CTAs per SM the tracker asks the register allocator for: the row of H_x (N
@@ -331,7 +469,7 @@ __host__ __device__ inline size_t sub_bytes(int N, int Mc, bool mixed = false, i
 template <int N, typename RS, typename RP>
 constexpr int track_min_blocks() {
   return (sizeof(RS) == 8 && sizeof(RP) == 8)
-             ? (N <= 4 ? 8 : N <= 8 ? 4 : N <= 12 ? 6 : N <= 18 ? 3 : 2)
+             ? (N <= 4 ? 8 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
              : (sizeof(RS) == 8 ? (N <= 4 ? 8 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
                                 : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 3));
 }
@@ -362,11 +500,14 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 //   RCL corrector precision for t < t_switch RCH corrector precision for t >= t_switch
 //
 // Each sub-warp runs its path as a small state machine (phase 0..3 = RK stage,
-// 4 = Newton iteration).  One trip of the warp loop performs exactly one
+// 4 = Newton iteration).  Mixed precision escalates a path after a failed step:
+// its next kEscalateSteps steps run predictor and corrector in RCH, so an
+// ill-conditioned stretch is not retried in low precision with ever smaller dt.  One trip of the warp loop performs exactly one
 // evaluate-and-solve for every sub-warp, whatever its phase, so the unrolled
 // LU exists once per precision in the code and sub-warps of one warp never
 // wait on each other's corrector iterations.
 // -------------------------------------------------------------------------------------------------
+constexpr int kEscalateSteps = 4;
 #ifdef GHC_TRACK_MIN_BLOCKS
 #define GHC_MINB(N, RS, RP) GHC_TRACK_MIN_BLOCKS
 #else
@@ -383,7 +524,9 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
   const int l = lane % W;
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
-  unsigned char* base = smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, kMixed, W);
+  const bool flat = kFlatAlways<N> || p.flat_eval;
+  unsigned char* base =
+      smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, kMixed, W, flat);
   SubMem sm;  // predictor / low-precision corrector buffers
   sm.coefA = base;
   sm.coefB = base + 16 * (size_t)Mc;
@@ -399,6 +542,9 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
   unsigned char* lane_state = (kMixed ? smh.coefB + 16 * (size_t)Mc : sm.sol + 16 * N) + 16 * (size_t)l;
   cx<RS>& x0 = *reinterpret_cast<cx<RS>*>(lane_state);
   cx<RS>& sols = *reinterpret_cast<cx<RS>*>(lane_state + 16 * W);
+  sm.scr = flat ? lane_state - 16 * (size_t)l + 32 * (size_t)W : nullptr;
+  smh.scr = sm.scr;
+  if (flat) zero_scratch<N, W>(sm.scr, l);
 
   const int subs_per_cta = blockDim.x / W;
   const long long n_sw = (long long)gridDim.x * subs_per_cta;
@@ -411,7 +557,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
   cx<RS> x = mk(RS(0), RS(0));
   RS t0 = 0, dt = 0, t_step = 0, half = 0;
   bool end_zone = false, success = false, inf = false, hi = false;
-  int nsucc = 0, step = 0, ncorr = 0, phase = 0, cit = 0;
+  int nsucc = 0, step = 0, ncorr = 0, phase = 0, cit = 0, esc = 0;
   const RS dt_init = (KIND == KIND_PH) ? RS(0.01) : RS(0.05);
 
   // end-zone clamp and bookkeeping at the start of a step (kernel_HC_Solver_P3P.cu:121-134)
@@ -449,6 +595,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
     nsucc = 0;
     step = 0;
     ncorr = 0;
+    esc = 0;
     prologue();
   };
   if (alive) init_path(item);
@@ -456,15 +603,15 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
   while (__any_sync(kFull, alive)) {
     // ---------------- which sub-warps are served this trip.  Mixed precision: one precision per
     // trip for the whole warp (the high-precision corrector first); the others wait one trip.
-    const bool want_hi = kMixed && alive && phase == 4 && hi;
+    const bool want_hi = kMixed && alive && (phase == 4 ? hi : esc > 0);
     const bool want_lo = alive && !want_hi;
     const bool serve_hi = kMixed && __any_sync(kFull, want_hi);
     const bool served = serve_hi ? want_hi : want_lo;
     const bool rk = served && phase < 4;
     const bool corr = served && phase == 4;
     // ---------------- coefficients: every RK stage at its t; the corrector reuses stage 4's
-    if (rk) coef_eval<RP, W, KIND>(p, sm, hyp, (RP)t0, l);
-    if (kMixed && corr && hi && cit == 0) coef_eval<RCH, W, KIND>(p, smh, hyp, (RCH)t0, l);
+    if (rk && !serve_hi) coef_eval<RP, W, KIND>(p, sm, hyp, (RP)t0, l);
+    if (kMixed && serve_hi && (rk || (corr && cit == 0))) coef_eval<RCH, W, KIND>(p, smh, hyp, (RCH)t0, l);
     // ---------------- one evaluate-and-solve per served sub-warp (predictor: -H_t, corrector: H)
     cx<RS> v = mk(RS(0), RS(0));
     if (!serve_hi) {
@@ -474,7 +621,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
     } else if (kMixed) {
       write_track<RCH, RS, N>(smh, l, x);
       __syncwarp(kFull);
-      v = c_cast<RS>(eval_solve<RCH, N, W, KIND>(tb, smh, l, 0));
+      v = c_cast<RS>(eval_solve<RCH, N, W, KIND>(tb, smh, l, rk ? 1 : 0));
     }
     // ---------------- corrector norms (kernel_HC_Solver_P3P.cu:204-219), all lanes take part
     RS ns0 = 0, nc0 = 0;
@@ -501,7 +648,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
         x = sols;
         phase = 4;
         cit = 0;
-        hi = kMixed && (double)t0 >= p.t_switch;
+        hi = kMixed && ((double)t0 >= p.t_switch || esc > 0);
         success = false;
         inf = false;
         if (p.max_corr <= 0) end_step = true;
@@ -520,12 +667,14 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
       if (inf) {
         done = true;
       } else if (!success) {
+        if (kMixed) esc = kEscalateSteps;
         dt = f_mul(dt, RS(0.5));
         x = x0;
         sols = x0;
         nsucc = 0;
         t0 = t_step;
       } else {
+        if (kMixed && esc > 0) --esc;
         ++nsucc;
         x0 = x;
         sols = x;
@@ -580,13 +729,17 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
   const int l = lane % W;
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
-  unsigned char* base = smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc);
+  const bool flat = kFlatAlways<N> || p.flat_eval;
+  unsigned char* base =
+      smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, false, W, flat);
   SubMem sm;
   sm.coefA = base;
   sm.coefB = base + 16 * (size_t)Mc;
   sm.xs = base + 32 * (size_t)Mc;
   sm.sx = sm.xs + 16 * (N + 1);
   sm.sol = sm.sx + 16 * (N + 1);
+  sm.scr = flat ? sm.sol + 16 * N + 32 * (size_t)W : nullptr;
+  if (flat) zero_scratch<N, W>(sm.scr, l);
   const int subs_per_cta = blockDim.x / W;
   const int leader = lane - l;
   for (long long item0 = (long long)blockIdx.x * subs_per_cta; item0 < p.n_items;
@@ -618,8 +771,8 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
     __syncwarp(kFull);
     cx<double> A[N];
     cx<double> h;
-    eval_row<double, N, KIND>(tb, view<double>(sm.coefA), view<double>(sm.coefB), view<double>(sm.xs), l, l < N, A,
-                              h, 0);
+    eval_row<double, N, W, KIND>(tb, view<double>(sm.coefA), view<double>(sm.coefB), view<double>(sm.xs), l, l < N, A,
+                                 h, 0, flat, sm.scr);
     const double s = tree_sum<double, N, W>(l < N ? c_abs2(h) : 0.0);
     const double s0 = __shfl_sync(kFull, s, leader);
     if (valid) {

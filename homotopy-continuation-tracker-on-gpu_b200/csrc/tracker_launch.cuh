@@ -19,7 +19,8 @@ int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
   const bool mixed = !std::is_same<RCL, RCH>::value;
-  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, mixed, W);
+  const bool flat = dev::kFlatAlways<N> || p.flat_eval;
+  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, mixed, W, flat);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return -20;
   int occ = 0;
@@ -43,7 +44,8 @@ int launch_polish_t(const PolishParams& p, cudaStream_t s) {
   auto kern = dev::polish_kernel<N, W, KIND>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
-  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc);
+  const bool flat = dev::kFlatAlways<N> || p.flat_eval;
+  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, false, W, flat);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -20;
   long long grid = (p.n_items + subs - 1) / subs;
   if (grid > 65535LL * 16) grid = 65535LL * 16;

@@ -12,6 +12,8 @@ mix      uneven mix in one graph launch: P3P_TD 8192, 5-point 4096,
 served   Poisson request stream through serve.Server (continuous batching).
 g3v4_mono  generalized 3-view with start parameters ~ complex N(0,1) and
          start solutions from the monodromy solver, plain FP64 vs mixed.
+problem  any problem folder (--problem), --hyp hypotheses per launch, one
+         precision (--precision) and step control (--step): the tracker alone.
 
 Each prints one JSON line with the bench contract's keys.
 """
@@ -63,7 +65,7 @@ class Batch:
         self.d_diff = _cx(tg - np.asarray(st)[None, :], torch)
         s0 = self.pb.start_sols() if sols is None else sols
         self.paths = s0.shape[0]
-        self.d_sols = _cx(s0, torch)
+        self.d_sols = _cx(s0, torch, torch.float32 if precision == ghc.PREC_FP32 else None)
         self.ws = ghc.Workspace(self.pb, H, precision, paths=self.paths)
         self.kw = dict(polish_iters=polish, want_resid=polish > 0, t_switch=0.0)
         if step:
@@ -255,6 +257,32 @@ def config_g3v4_mono(args, torch):
           ground_truth_found_frac=gt_hits / H, monodromy={"solutions": len(S), "seconds": mono_s})
 
 
+def config_problem(args, torch):
+    prec = {"fp64": ghc.PREC_FP64, "fp32": ghc.PREC_FP32, "mixed": ghc.PREC_MIXED}[args.precision]
+    step = None
+    if args.step == "robust":
+        step = dict(step=dict(corr_tol2=1e-12, first_tol2=1e-2, dt_max=0.05), max_corr=3, max_steps=2000)
+    H = args.hyp
+    b = Batch(torch, args.problem, H, 500 + args.seed, precision=prec, step=step)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    g = _capture(torch, b.launch)
+    for _ in range(args.warmup):
+        g.replay()
+    ms = _time_graph(torch, g, args.steps, flush)
+    steps = b.ws.steps.cpu().numpy().astype(np.int64)
+    solves = 4 * steps + b.ws.corr.cpu().numpy()
+    total = sum(ms)
+    _line("hypothesis-solves/s (one problem, batched)", H * len(ms) / (total * 1e-3), args,
+          {"workload": "%s: %d hypotheses x %d paths per launch, %s, %s step control, one CUDA graph"
+                       % (args.problem, H, b.paths, args.precision, args.step), "l2": "flushed before each step"},
+          ms_per_step=total / len(ms), p50_ms=float(np.percentile(ms, 50)),
+          paths={"per_step": H * b.paths, "converged_frac": float(b.ws.conv.float().mean()),
+                 "mean_solves": float(solves.mean()), "p99_solves": float(np.percentile(solves, 99)),
+                 "max_solves": int(solves.max())},
+          solves_per_s=float(solves.sum()) / (statistics.median(ms) * 1e-3), gpu_launches=len(ms) * (2 if
+          b.pb.kind == ghc.KIND_P2C else 1))
+
+
 def config_served(args, torch):
     import serve
     serve.bench(args, torch)
@@ -264,4 +292,4 @@ def run(args):
     import torch
     torch.cuda.set_device(0)
     {"cy": config_cy, "p3p_td": config_p3p_td, "mix": config_mix, "served": config_served,
-     "g3v4_mono": config_g3v4_mono}[args.config](args, torch)
+     "g3v4_mono": config_g3v4_mono, "problem": config_problem}[args.config](args, torch)

@@ -380,9 +380,9 @@ def secondary_modes(pb, ghc, cx, d_start, d_sols, scenes, dev, args):
     d_tg2 = cx(tg2)
     out = {}
     runs = {}
-    configs = [("fp64_ref", ghc.PREC_FP64, {}, 0), ("mixed_ref", ghc.PREC_MIXED, dict(t_switch=0.0), 0),
+    configs = [("fp64_ref", ghc.PREC_FP64, {}, 0), ("mixed_ref", ghc.PREC_MIXED, dict(t_switch=0.9), 0),
                ("fp64_robust", ghc.PREC_FP64, dict(step=ROBUST, max_corr=3, max_steps=2000), 3),
-               ("mixed_robust", ghc.PREC_MIXED, dict(step=ROBUST, max_corr=3, max_steps=2000, t_switch=0.0), 3)]
+               ("mixed_robust", ghc.PREC_MIXED, dict(step=ROBUST, max_corr=3, max_steps=2000, t_switch=0.9), 3)]
     for name, prec, kw, pol in configs:
         ws = ghc.Workspace(pb, H2, prec)
         hx, ht = pb.p2c_device(d_start, d_tg2)

@@ -52,6 +52,10 @@ int track_code(int rc) {
     set_error("unknown precision mode");
     return GHC_ERR_ARG;
   }
+  if (rc == -12) {
+    set_error("mixed precision needs d_steps, d_corr, d_t_end and d_dt_end (the FP32 -> FP64 handover state)");
+    return GHC_ERR_ARG;
+  }
   return cuda_fail("tracker launch");
 }
 
@@ -73,7 +77,6 @@ TrackParams base_params(const Problem& pb) {
   p.ht_terms = pb.dev.ht_terms;
   p.ht_off = pb.dev.ht_off;
   p.flat_eval = flat_eval_pays(pb.hx_off.data(), pb.N);
-  p.t_switch = 2.0;
   // the reference's step control (kernel_HC_Solver_P3P.cu:214): no contraction test, no step cap
   p.corr_tol2 = 1e-6;
   p.first_tol2 = HUGE_VAL;
@@ -248,7 +251,7 @@ double dropin(const ghc_problem* h, void* stream, int max_steps, int max_corr, i
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
-  rc = track_code(launch_track(p, fp32 ? PREC_FP32 : PREC_FP64, stream, sm_count()));
+  rc = track_code(launch_track(p, fp32 ? PREC_FP32 : PREC_FP64, 0.0, stream, sm_count()));
   cudaEventRecord(e1, st);
   if (!rc && d_debug) {
     if (fp32) rc = launch_debug_f(d_conv, d_t, d_dt, (float*)d_debug, n, stream);
@@ -431,12 +434,10 @@ int ghc_track(const ghc_problem* h, const ghc_track_args* a, void* stream) {
   p.t_end = a->d_t_end;
   p.dt_end = a->d_dt_end;
   p.counter = a->d_counter;
-  p.t_switch = a->t_switch;
-  if (a->precision == GHC_PREC_FP64) p.t_switch = 2.0;
   if (a->corr_tol2 > 0) p.corr_tol2 = a->corr_tol2;
   if (a->first_tol2 > 0) p.first_tol2 = a->first_tol2;
   if (a->dt_max > 0) p.dt_max = a->dt_max;
-  rc = track_code(launch_track(p, a->precision, stream, sm_count()));
+  rc = track_code(launch_track(p, a->precision, a->t_switch, stream, sm_count()));
   if (rc) return rc;
   const bool fp64_state = a->precision == GHC_PREC_FP64 || a->precision == GHC_PREC_MIXED;
   if ((a->polish_iters > 0 || a->d_resid) && fp64_state) {
@@ -579,8 +580,9 @@ int ghc_solve_host(const ghc_problem* h, int32_t precision, int64_t n_hyp, const
   double* d_ht = pb.kind == KIND_P2C ? (double*)dmalloc(std::max(nht, 1LL) * n_hyp * sizeof(double)) : nullptr;
   void* d_ep = dmalloc(2 * (size_t)n * N * rs);
   uint8_t* d_flags = (uint8_t*)dmalloc(3 * (size_t)n);
-  int32_t* d_steps = (int32_t*)dmalloc((size_t)n * 4 + 16);
-  if (!d_start || !d_ps || !d_tg || !d_pd || !d_ep || !d_flags || !d_steps ||
+  int32_t* d_steps = (int32_t*)dmalloc((size_t)n * 8 + 16);  // steps, corrector iterations
+  double* d_tdt = (double*)dmalloc((size_t)n * 16 + 16);       // t_end, dt_end
+  if (!d_start || !d_ps || !d_tg || !d_pd || !d_ep || !d_flags || !d_steps || !d_tdt ||
       (pb.kind == KIND_P2C && (!d_hx || !d_ht)))
     return cuda_fail("allocation");
   if (pb.kind == KIND_P2C && !pb.has_terms) {
@@ -625,6 +627,9 @@ int ghc_solve_host(const ghc_problem* h, int32_t precision, int64_t n_hyp, const
   a.d_conv = d_flags + n;
   a.d_inf = d_flags + 2 * n;
   a.d_steps = d_steps;
+  a.d_corr = d_steps + n;
+  a.d_t_end = d_tdt;
+  a.d_dt_end = d_tdt + n;
   a.d_counter = pb.dev.counter;
   if (!rc) rc = ghc_track(h, &a, st);
   cudaEventRecord(ev[2], st);

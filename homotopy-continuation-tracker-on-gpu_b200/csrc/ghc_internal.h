@@ -83,6 +83,13 @@ struct TrackParams {
   int ld_start;
   const void* track_in;    // optional initial track [n_items][ld_track] (nullptr -> start_sols)
   int ld_track;
+  int start_other;         // start_sols / track_in hold the other precision than the kernel's
+  int track_other;         //   (double for the FP32 tracker, float for the FP64 tracker)
+  // resuming: per item start t and step (nullptr -> 0 and the initial step), and the
+  // step / corrector counts already in steps / corr
+  const double* t_in;
+  const double* dt_in;
+  int resume;
   const double* coef_hx;   // P2C [n_hyp][(M+1)(K+1)] complex double
   long long stride_hx;     // in complex entries (0 -> shared by all hypotheses)
   const double* coef_ht;   // P2C [n_hyp][(M+1)K]
@@ -103,8 +110,10 @@ struct TrackParams {
   double* dt_end;
   // scratch
   int* counter;            // one int, zero before launch
-  // mixed precision: corrector in the high precision once t >= t_switch
-  double t_switch;
+  // handover (first phase of mixed precision): stop at t_handover (> 0) or after
+  // fail_limit (> 0) consecutive failed steps or on divergence, keeping the last accepted point
+  double t_handover;
+  int fail_limit;
   // step control (reference: corr_tol2 = 1e-6, first_tol2 = dt_max = +inf)
   double corr_tol2;   // corrector success: |dx|^2 < corr_tol2 |x|^2
   double first_tol2;  // reject when the first Newton update has |dx|^2 > first_tol2 |x|^2
@@ -154,7 +163,9 @@ struct P2CParams {
 };
 
 // launch entry points implemented in tracker.cu / p2c.cu
-int launch_track(const TrackParams& p, int precision, void* stream, int n_sm);
+// precision PREC_MIXED runs two launches (FP32 to t_switch with handover, then FP64) and
+// needs p.steps, p.corr, p.t_end and p.dt_end; t_switch is ignored by the other modes.
+int launch_track(const TrackParams& p, int precision, double t_switch, void* stream, int n_sm);
 int launch_polish(const PolishParams& p, void* stream);
 int launch_p2c(const P2CParams& p, void* stream);
 int track_subwarp_width(int N);

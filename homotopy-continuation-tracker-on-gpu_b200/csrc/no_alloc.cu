@@ -169,20 +169,23 @@ extern "C" int ghc_track_noalloc(const ghc_problem* h, const ghc_track_args* a, 
   p.t_end = a->d_t_end;
   p.dt_end = a->d_dt_end;
   p.counter = reinterpret_cast<int*>(s);  // cleared on `stream` by the launch
-  p.t_switch = a->precision == GHC_PREC_FP64 ? 2.0 : a->t_switch;
   p.corr_tol2 = a->corr_tol2 > 0 ? a->corr_tol2 : 1e-6;
   p.first_tol2 = a->first_tol2 > 0 ? a->first_tol2 : HUGE_VAL;
   p.dt_max = a->dt_max > 0 ? a->dt_max : HUGE_VAL;
   int dev = 0, n_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  rc = launch_track(p, a->precision, stream, n_sm > 0 ? n_sm : 1);
+  rc = launch_track(p, a->precision, a->t_switch, stream, n_sm > 0 ? n_sm : 1);
   if (rc == -10) {
     set_error("system size or kind has no compiled tracker");
     return GHC_ERR_RANGE;
   }
   if (rc == -11) {
     set_error("unknown precision mode");
+    return GHC_ERR_ARG;
+  }
+  if (rc == -12) {
+    set_error("mixed precision needs d_steps, d_corr, d_t_end and d_dt_end (the FP32 -> FP64 handover state)");
     return GHC_ERR_ARG;
   }
   if (rc) {

@@ -47,6 +47,11 @@ __device__ __forceinline__ double f_div(double a, double b) { return __ddiv_rn(a
 __device__ __forceinline__ float f_div(float a, float b) { return __fdiv_rn(a, b); }
 
 template <typename R>
+__device__ __forceinline__ cx<R>* view(unsigned char* p) {
+  return reinterpret_cast<cx<R>*>(p);
+}
+
+template <typename R>
 __device__ __forceinline__ cx<R> mk(R a, R b) {
   cx<R> r;
   r.re = a;
@@ -170,7 +175,7 @@ __device__ __forceinline__ cx<R> term_coef_value(uint64_t w, const cx<R>* ca) {
 // the row's terms are walked as one list (CSR row r, column in the term word),
 // so a sub-warp spends max_r(terms of row r) iterations instead of
 // sum_i max_r(terms of entry (r, i)).  Each entry's sum is staged in the
-// sub-warp's scratch row scr[i][r] (16-byte slots) and read back into
+// sub-warp's scratch row scr[i][r] and read back into
 // registers; entries without terms are never written and stay zero from the
 // kernel's start.  Entry-wise: one loop per column, straight into registers.
 // Either way every entry is summed in table order, as in the oracle.
@@ -181,7 +186,7 @@ template <typename R, int N, int W, int KIND>
 __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, const cx<R>* cb, const cx<R>* xs, int r,
                                          bool live, cx<R> (&A)[N], cx<R>& b, int which, bool flat,
                                          unsigned char* scr) {
-  auto slot = [&](int i) -> cx<R>* { return reinterpret_cast<cx<R>*>(scr + 16 * (size_t)(i * W + r)); };
+  auto slot = [&](int i) -> cx<R>* { return view<R>(scr) + (i * W + r); };
   if (!kFlatAlways<N> && !flat) {
 #pragma unroll
     for (int i = 0; i < N; ++i) {
@@ -404,16 +409,12 @@ __device__ __forceinline__ R tree_sum(R v) {
 struct SubMem {
   unsigned char* coefA;  // c_k(t)   or p(t)     [Mc]
   unsigned char* coefB;  // c'_k(t)  or p1 - p0  [Mc]
-  unsigned char* xs;     // track in stage precision [N+1]
+  unsigned char* xs;     // track [N+1]
   unsigned char* sx;     // pivot row + rhs [N+1]
   unsigned char* sol;    // solution [N]
-  unsigned char* scr;    // H_x row scratch [N][W] 16-byte slots (both precisions), null unless flat
+  unsigned char* state;  // per lane: RK base point x0 [W], RK accumulator [W]
+  unsigned char* scr;    // H_x row scratch [N][W], null unless the evaluation is flat
 };
-
-template <typename R>
-__device__ __forceinline__ cx<R>* view(unsigned char* p) {
-  return reinterpret_cast<cx<R>*>(p);
-}
 
 // one evaluation + solve in precision R; returns this lane's solution component
 template <typename R, int N, int W, int KIND>
@@ -427,10 +428,10 @@ __device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, 
   return k;
 }
 
-template <typename R, typename RS, int N>
-__device__ __forceinline__ void write_track(const SubMem& sm, int l, cx<RS> x) {
+template <typename R, int N>
+__device__ __forceinline__ void write_track(const SubMem& sm, int l, cx<R> x) {
   cx<R>* xs = view<R>(sm.xs);
-  if (l < N) xs[l] = c_cast<R>(x);
+  if (l < N) xs[l] = x;
   if (l == 0) xs[N] = mk(R(1), R(0));
 }
 
@@ -450,28 +451,50 @@ __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t
 __host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
   return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(N * N + 1 + N + 1));
 }
-// per sub-warp: coefficient buffers (two sets when mixed), track, pivot row, solution,
-// two lane-state slots per lane, the H_x scratch row [N][W] when the evaluation is flat
-__host__ __device__ inline size_t sub_bytes(int N, int Mc, bool mixed, int W, bool flat) {
-  return align16(16 * (size_t)(2 * Mc * (mixed ? 2 : 1) + (N + 1) + (N + 1) + N + 2 * W + (flat ? N * W : 0)));
+// per sub-warp, in complex values of esz bytes: coefficient buffers [2 Mc], track and
+// pivot row [2 (N+1)], solution [N], lane state [2 W], scratch row [N W] when flat
+__host__ __device__ inline size_t sub_bytes(int N, int Mc, int W, bool flat, int esz) {
+  return align16((size_t)esz * (2 * (size_t)Mc + 2 * (N + 1) + N + 2 * W + (flat ? N * W : 0)));
+}
+template <typename R>
+__device__ __forceinline__ SubMem sub_layout(unsigned char* base, int N, int Mc, int W, bool flat) {
+  constexpr int e = sizeof(cx<R>);
+  SubMem sm;
+  sm.coefA = base;
+  sm.coefB = base + e * (size_t)Mc;
+  sm.xs = base + 2 * e * (size_t)Mc;
+  sm.sx = sm.xs + e * (N + 1);
+  sm.sol = sm.sx + e * (N + 1);
+  sm.state = sm.sol + e * N;
+  sm.scr = flat ? sm.state + 2 * e * W : nullptr;
+  return sm;
 }
 
 // zero this lane's slots of the scratch row (lane l owns slots i*W + l)
-template <int N, int W>
+template <typename R, int N, int W>
 __device__ __forceinline__ void zero_scratch(unsigned char* scr, int l) {
 #pragma unroll
-  for (int i = 0; i < N; ++i) *reinterpret_cast<double2*>(scr + 16 * (size_t)(i * W + l)) = make_double2(0.0, 0.0);
+  for (int i = 0; i < N; ++i) view<R>(scr)[i * W + l] = mk(R(0), R(0));
+}
+
+// complex entry idx of an array of doubles (f64) or floats, in precision R
+template <typename R>
+__device__ __forceinline__ cx<R> load_cx(const void* base, bool f64, long long idx) {
+  if (f64) {
+    const double* d = reinterpret_cast<const double*>(base) + 2 * idx;
+    return mk((R)d[0], (R)d[1]);
+  }
+  const float* f = reinterpret_cast<const float*>(base) + 2 * idx;
+  return mk((R)f[0], (R)f[1]);
 }
 
 // CTAs per SM the tracker asks the register allocator for: the row of H_x (N
 // complex values) dominates the registers, so small systems afford more.
-// Measured on B200 (FP64): N = 3 best at 8, N = 6 at 4, N = 12 at 6; mixed N = 12 at 4.
-template <int N, typename RS, typename RP>
+// Measured on B200: FP64 N = 3 best at 8, N = 6 and N = 12 at 4.
+template <int N, typename R>
 constexpr int track_min_blocks() {
-  return (sizeof(RS) == 8 && sizeof(RP) == 8)
-             ? (N <= 4 ? 8 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
-             : (sizeof(RS) == 8 ? (N <= 4 ? 8 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
-                                : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 3));
+  return sizeof(R) == 8 ? (N <= 4 ? 8 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
+                        : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 3);
 }
 
 __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64_t* g_hx, const uint16_t* g_hxo,
@@ -495,28 +518,28 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 }
 
 // -------------------------------------------------------------------------------------------------
-// the tracker kernel
-//   RS  state precision (track, t, dt)      RP  predictor (RK) precision
-//   RCL corrector precision for t < t_switch RCH corrector precision for t >= t_switch
+// the tracker kernel, one precision R for the whole path
 //
 // Each sub-warp runs its path as a small state machine (phase 0..3 = RK stage,
-// 4 = Newton iteration).  Mixed precision escalates a path after a failed step:
-// its next kEscalateSteps steps run predictor and corrector in RCH, so an
-// ill-conditioned stretch is not retried in low precision with ever smaller dt.  One trip of the warp loop performs exactly one
+// 4 = Newton iteration).  One trip of the warp loop performs exactly one
 // evaluate-and-solve for every sub-warp, whatever its phase, so the unrolled
-// LU exists once per precision in the code and sub-warps of one warp never
-// wait on each other's corrector iterations.
+// LU exists once in the code and sub-warps of one warp never wait on each
+// other's corrector iterations.
+//
+// Handover (first phase of the mixed-precision mode: t_handover > 0 or
+// fail_limit > 0): a path also stops when t reaches t_handover, after
+// fail_limit consecutive failed steps, or when the corrector sees divergence,
+// leaving its last accepted point, t and dt in endpoints / t_end / dt_end.
+// A resuming launch (resume = 1) starts every item from track_in at t_in[i]
+// with step dt_in[i] and the step / corrector counts already in steps / corr.
 // -------------------------------------------------------------------------------------------------
-constexpr int kEscalateSteps = 4;
 #ifdef GHC_TRACK_MIN_BLOCKS
-#define GHC_MINB(N, RS, RP) GHC_TRACK_MIN_BLOCKS
+#define GHC_MINB(N, R) GHC_TRACK_MIN_BLOCKS
 #else
-#define GHC_MINB(N, RS, RP) track_min_blocks<N, RS, RP>()
+#define GHC_MINB(N, R) track_min_blocks<N, R>()
 #endif
-template <typename RS, typename RP, typename RCL, typename RCH, int N, int W, int KIND>
-__global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const TrackParams p) {
-  static_assert(std::is_same<RP, RCL>::value, "the low-precision corrector shares the predictor's buffers");
-  constexpr bool kMixed = !std::is_same<RCL, RCH>::value;
+template <typename R, int N, int W, int KIND>
+__global__ void __launch_bounds__(128, GHC_MINB(N, R)) track_kernel(const TrackParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Tables tb = stage_tables(smem, p.hx_terms, p.hx_off, p.ht_terms, p.ht_off, N, p.n_hx_terms, p.n_ht_terms);
 
@@ -525,110 +548,97 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const bool flat = kFlatAlways<N> || p.flat_eval;
-  unsigned char* base =
-      smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, kMixed, W, flat);
-  SubMem sm;  // predictor / low-precision corrector buffers
-  sm.coefA = base;
-  sm.coefB = base + 16 * (size_t)Mc;
-  sm.xs = base + 32 * (size_t)Mc;
-  sm.sx = sm.xs + 16 * (N + 1);
-  sm.sol = sm.sx + 16 * (N + 1);
-  SubMem smh = sm;  // high-precision corrector: own coefficient buffers
-  if (kMixed) {
-    smh.coefA = sm.sol + 16 * N;
-    smh.coefB = smh.coefA + 16 * (size_t)Mc;
-  }
+  const SubMem sm = sub_layout<R>(smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) +
+                                      (size_t)g * sub_bytes(N, Mc, W, flat, (int)sizeof(cx<R>)),
+                                  N, Mc, W, flat);
   // this lane's RK base point x0 and accumulator sols live in shared memory (register relief)
-  unsigned char* lane_state = (kMixed ? smh.coefB + 16 * (size_t)Mc : sm.sol + 16 * N) + 16 * (size_t)l;
-  cx<RS>& x0 = *reinterpret_cast<cx<RS>*>(lane_state);
-  cx<RS>& sols = *reinterpret_cast<cx<RS>*>(lane_state + 16 * W);
-  sm.scr = flat ? lane_state - 16 * (size_t)l + 32 * (size_t)W : nullptr;
-  smh.scr = sm.scr;
-  if (flat) zero_scratch<N, W>(sm.scr, l);
+  cx<R>& x0 = view<R>(sm.state)[l];
+  cx<R>& sols = view<R>(sm.state)[W + l];
+  if (flat) zero_scratch<R, N, W>(sm.scr, l);
 
   const int subs_per_cta = blockDim.x / W;
   const long long n_sw = (long long)gridDim.x * subs_per_cta;
   const int leader = lane - l;
+  const bool handover = p.t_handover > 0.0 || p.fail_limit > 0;
+  const R t_hand = (R)p.t_handover;
 
   // per-path state (replicated across the sub-warp's lanes)
   long long item = (long long)blockIdx.x * subs_per_cta + g;
   bool alive = item < p.n_items;
   long long hyp = 0;
-  cx<RS> x = mk(RS(0), RS(0));
-  RS t0 = 0, dt = 0, t_step = 0, half = 0;
-  bool end_zone = false, success = false, inf = false, hi = false;
-  int nsucc = 0, step = 0, ncorr = 0, phase = 0, cit = 0, esc = 0;
-  const RS dt_init = (KIND == KIND_PH) ? RS(0.01) : RS(0.05);
+  cx<R> x = mk(R(0), R(0));
+  R t0 = 0, dt = 0, t_step = 0, half = 0, dt_pre = 0;
+  bool end_zone = false, success = false, inf = false, finished = false;
+  int nsucc = 0, step = 0, ncorr = 0, phase = 0, cit = 0, nfail = 0;
+  const R dt_init = (KIND == KIND_PH) ? R(0.01) : R(0.05);
 
   // end-zone clamp and bookkeeping at the start of a step (kernel_HC_Solver_P3P.cu:121-134)
   auto prologue = [&]() {
-    if (!end_zone && fabs(f_sub(RS(1), t0)) <= RS(0.0500001)) end_zone = true;
+    if (!end_zone && fabs(f_sub(R(1), t0)) <= R(0.0500001)) end_zone = true;
     if (end_zone) {
-      const RS rem = fabs(f_sub(RS(1), t0));
+      const R rem = fabs(f_sub(R(1), t0));
       if (dt > rem) dt = rem;
     } else {
-      const RS edge = (KIND == KIND_PH) ? fabs(f_sub(RS(0.95), t0)) : fabs(f_sub(f_sub(RS(1), RS(0.05)), t0));
+      const R edge = (KIND == KIND_PH) ? fabs(f_sub(R(0.95), t0)) : fabs(f_sub(f_sub(R(1), R(0.05)), t0));
       if (dt > edge) dt = edge;
     }
+    dt_pre = dt;  // the step without the handover clamp: the next phase resumes with it
+    if (p.t_handover > 0.0 && dt > f_sub(t_hand, t0)) dt = f_sub(t_hand, t0);
     t_step = t0;
-    half = f_mul(RS(0.5), dt);
+    half = f_mul(R(0.5), dt);
     phase = 0;
     cit = 0;
+  };
+  // the path stops before its next step (kernel_HC_Solver_P3P.cu:247-249, plus the handover rules)
+  auto at_end = [&]() -> bool {
+    return !(t0 < R(1) && f_sub(R(1), t0) > R(1e-7)) || step > p.max_steps ||
+           (p.t_handover > 0.0 && f_sub(t_hand, t0) <= R(1e-6)) || (p.fail_limit > 0 && nfail >= p.fail_limit);
   };
   auto init_path = [&](long long it) {
     hyp = it / p.paths_per_hyp;
     const long long pidx = it % p.paths_per_hyp;
-    const RS* st = reinterpret_cast<const RS*>(p.start_sols) + 2 * pidx * p.ld_start;
-    const RS* tr = p.track_in ? reinterpret_cast<const RS*>(p.track_in) + 2 * it * p.ld_track : st;
     if (l < N) {
-      sols = mk(st[2 * l], st[2 * l + 1]);
-      x = mk(tr[2 * l], tr[2 * l + 1]);
+      if (p.track_in) {
+        x = load_cx<R>(p.track_in, (sizeof(R) == 8) != (p.track_other != 0), it * p.ld_track + l);
+      } else {
+        x = load_cx<R>(p.start_sols, (sizeof(R) == 8) != (p.start_other != 0), pidx * p.ld_start + l);
+      }
     } else {
-      sols = x = mk(RS(0), RS(0));
+      x = mk(R(0), R(0));
     }
     x0 = x;
-    t0 = 0;
-    dt = dt_init;
+    sols = x;
+    t0 = p.t_in ? (R)p.t_in[it] : R(0);
+    dt = p.dt_in ? (R)p.dt_in[it] : dt_init;
+    dt_pre = dt;
+    step = p.resume ? p.steps[it] : 0;
+    ncorr = p.resume ? p.corr[it] : 0;
     end_zone = false;
     success = false;
     inf = false;
     nsucc = 0;
-    step = 0;
-    ncorr = 0;
-    esc = 0;
-    prologue();
+    nfail = 0;
+    finished = at_end();
+    if (!finished) prologue();
   };
   if (alive) init_path(item);
 
   while (__any_sync(kFull, alive)) {
-    // ---------------- which sub-warps are served this trip.  Mixed precision: one precision per
-    // trip for the whole warp (the high-precision corrector first); the others wait one trip.
-    const bool want_hi = kMixed && alive && (phase == 4 ? hi : esc > 0);
-    const bool want_lo = alive && !want_hi;
-    const bool serve_hi = kMixed && __any_sync(kFull, want_hi);
-    const bool served = serve_hi ? want_hi : want_lo;
+    const bool served = alive && !finished;
     const bool rk = served && phase < 4;
     const bool corr = served && phase == 4;
     // ---------------- coefficients: every RK stage at its t; the corrector reuses stage 4's
-    if (rk && !serve_hi) coef_eval<RP, W, KIND>(p, sm, hyp, (RP)t0, l);
-    if (kMixed && serve_hi && (rk || (corr && cit == 0))) coef_eval<RCH, W, KIND>(p, smh, hyp, (RCH)t0, l);
-    // ---------------- one evaluate-and-solve per served sub-warp (predictor: -H_t, corrector: H)
-    cx<RS> v = mk(RS(0), RS(0));
-    if (!serve_hi) {
-      write_track<RP, RS, N>(sm, l, x);
-      __syncwarp(kFull);
-      v = c_cast<RS>(eval_solve<RP, N, W, KIND>(tb, sm, l, rk ? 1 : 0));
-    } else if (kMixed) {
-      write_track<RCH, RS, N>(smh, l, x);
-      __syncwarp(kFull);
-      v = c_cast<RS>(eval_solve<RCH, N, W, KIND>(tb, smh, l, rk ? 1 : 0));
-    }
+    if (rk) coef_eval<R, W, KIND>(p, sm, hyp, t0, l);
+    // ---------------- one evaluate-and-solve per sub-warp (predictor: -H_t, corrector: H)
+    write_track<R, N>(sm, l, x);
+    __syncwarp(kFull);
+    const cx<R> v = eval_solve<R, N, W, KIND>(tb, sm, l, rk ? 1 : 0);
     // ---------------- corrector norms (kernel_HC_Solver_P3P.cu:204-219), all lanes take part
-    RS ns0 = 0, nc0 = 0;
+    R ns0 = 0, nc0 = 0;
     if (__any_sync(kFull, corr)) {
-      const cx<RS> xn = c_sub(x, v);
-      const RS ns = tree_sum<RS, N, W>((corr && l < N) ? c_abs2(v) : RS(0));
-      const RS nc = tree_sum<RS, N, W>((corr && l < N) ? c_abs2(xn) : RS(0));
+      const cx<R> xn = c_sub(x, v);
+      const R ns = tree_sum<R, N, W>((corr && l < N) ? c_abs2(v) : R(0));
+      const R nc = tree_sum<R, N, W>((corr && l < N) ? c_abs2(xn) : R(0));
       ns0 = __shfl_sync(kFull, ns, leader);
       nc0 = __shfl_sync(kFull, nc, leader);
     }
@@ -636,19 +646,18 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
     bool end_step = false;
     if (rk) {
       if (phase < 3) {
-        const RS a = f_mul(dt, phase == 0 ? RS(1.0 / 6.0) : RS(2.0 / 6.0));
-        const RS d = f_mul(dt, phase == 2 ? RS(1.0) : RS(0.5));
+        const R a = f_mul(dt, phase == 0 ? R(1.0 / 6.0) : R(2.0 / 6.0));
+        const R d = f_mul(dt, phase == 2 ? R(1.0) : R(0.5));
         sols = mk(f_fma(v.re, a, sols.re), f_fma(v.im, a, sols.im));
         x = mk(f_fma(v.re, d, x0.re), f_fma(v.im, d, x0.im));
         if (phase != 1) t0 = f_add(t0, half);
         ++phase;
       } else {
-        const RS a = f_mul(dt, RS(1.0 / 6.0));
+        const R a = f_mul(dt, R(1.0 / 6.0));
         sols = mk(f_fma(v.re, a, sols.re), f_fma(v.im, a, sols.im));
         x = sols;
         phase = 4;
         cit = 0;
-        hi = kMixed && ((double)t0 >= p.t_switch || esc > 0);
         success = false;
         inf = false;
         if (p.max_corr <= 0) end_step = true;
@@ -661,43 +670,50 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, RS, RP)) track_kernel(const T
       inf = ((double)nc0 > 1e14);
       end_step = inf || success || cit >= p.max_corr || (cit == 1 && (double)ns0 > p.first_tol2 * (double)nc0);
     }
-    bool done = false;
+    bool done = alive && finished;
     if (end_step) {
       // step control (kernel_HC_Solver_P3P.cu:225-249)
       if (inf) {
+        if (handover) {  // hand the last accepted point over
+          x = x0;
+          t0 = t_step;
+        }
         done = true;
       } else if (!success) {
-        if (kMixed) esc = kEscalateSteps;
-        dt = f_mul(dt, RS(0.5));
+        dt = f_mul(dt, R(0.5));
         x = x0;
         sols = x0;
         nsucc = 0;
         t0 = t_step;
+        ++nfail;
       } else {
-        if (kMixed && esc > 0) --esc;
+        nfail = 0;
         ++nsucc;
         x0 = x;
         sols = x;
         if (nsucc >= p.incr) {
           nsucc = 0;
-          dt = f_mul(dt, RS(2));
-          if ((double)dt > p.dt_max) dt = (RS)p.dt_max;
+          dt = f_mul(dt, R(2));
+          if ((double)dt > p.dt_max) dt = (R)p.dt_max;
         }
       }
       ++step;
-      if (!done) done = !(t0 < RS(1) && f_sub(RS(1), t0) > RS(1e-7)) || step > p.max_steps;
+      if (!done) done = at_end();
+      if (done && !inf && p.t_handover > 0.0 && f_sub(t_hand, t0) <= R(1e-6) && step <= p.max_steps &&
+          dt < dt_pre)
+        dt = dt_pre;
       if (!done) prologue();
     }
 
     // ---------------- finished paths: write out and take the next path
     if (done) {
-      RS* ep = reinterpret_cast<RS*>(p.endpoints) + 2 * item * p.ld_out;
+      R* ep = reinterpret_cast<R*>(p.endpoints) + 2 * item * p.ld_out;
       if (l < N) {
         ep[2 * l] = x.re;
         ep[2 * l + 1] = x.im;
       }
       if (l == 0) {
-        const bool conv = (t0 >= RS(1) || f_sub(RS(1), t0) <= RS(1e-7));
+        const bool conv = (t0 >= R(1) || f_sub(R(1), t0) <= R(1e-7));
         if (p.conv) p.conv[item] = conv ? 1 : 0;
         if (p.infy) p.infy[item] = inf ? 1 : 0;
         if (p.status) p.status[item] = conv ? ST_CONVERGED : (inf ? ST_DIVERGED : ST_STEP_CAP);
@@ -730,16 +746,9 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const bool flat = kFlatAlways<N> || p.flat_eval;
-  unsigned char* base =
-      smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, false, W, flat);
-  SubMem sm;
-  sm.coefA = base;
-  sm.coefB = base + 16 * (size_t)Mc;
-  sm.xs = base + 32 * (size_t)Mc;
-  sm.sx = sm.xs + 16 * (N + 1);
-  sm.sol = sm.sx + 16 * (N + 1);
-  sm.scr = flat ? sm.sol + 16 * N + 32 * (size_t)W : nullptr;
-  if (flat) zero_scratch<N, W>(sm.scr, l);
+  const SubMem sm = sub_layout<double>(
+      smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, W, flat, 16), N, Mc, W, flat);
+  if (flat) zero_scratch<double, N, W>(sm.scr, l);
   const int subs_per_cta = blockDim.x / W;
   const int leader = lane - l;
   for (long long item0 = (long long)blockIdx.x * subs_per_cta; item0 < p.n_items;
@@ -761,13 +770,13 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
     }
     __syncwarp(kFull);
     for (int it = 0; it < p.iters; ++it) {
-      write_track<double, double, N>(sm, l, x);
+      write_track<double, N>(sm, l, x);
       __syncwarp(kFull);
       const cx<double> d = eval_solve<double, N, W, KIND>(tb, sm, l, 0);
       if (conv) x = c_sub(x, d);
     }
     // residual |H(x,1)|
-    write_track<double, double, N>(sm, l, x);
+    write_track<double, N>(sm, l, x);
     __syncwarp(kFull);
     cx<double> A[N];
     cx<double> h;

@@ -3,6 +3,6 @@
 
 namespace ghc {
 int launch_track_fp32(const TrackParams& p, cudaStream_t s, int n_sm) {
-  return launch_mode<float, float, float, float>(p, s, n_sm);
+  return launch_mode<float>(p, s, n_sm);
 }
 }  // namespace ghc

@@ -3,6 +3,6 @@
 
 namespace ghc {
 int launch_track_fp64(const TrackParams& p, cudaStream_t s, int n_sm) {
-  return launch_mode<double, double, double, double>(p, s, n_sm);
+  return launch_mode<double>(p, s, n_sm);
 }
 }  // namespace ghc

@@ -2,8 +2,6 @@
 #pragma once
 #include <cuda_runtime.h>
 
-#include <type_traits>
-
 #include "ghc_internal.h"
 #include "tracker.cuh"
 
@@ -12,15 +10,15 @@ namespace launch_detail {
 
 constexpr int kBlock = 128;
 
-template <typename RS, typename RP, typename RCL, typename RCH, int N, int KIND>
+template <typename R, int N, int KIND>
 int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
   constexpr int W = (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
-  auto kern = dev::track_kernel<RS, RP, RCL, RCH, N, W, KIND>;
+  auto kern = dev::track_kernel<R, N, W, KIND>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
-  const bool mixed = !std::is_same<RCL, RCH>::value;
   const bool flat = dev::kFlatAlways<N> || p.flat_eval;
-  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, mixed, W, flat);
+  const size_t smem =
+      dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, flat, 2 * (int)sizeof(R));
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return -20;
   int occ = 0;
@@ -45,7 +43,7 @@ int launch_polish_t(const PolishParams& p, cudaStream_t s) {
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
   const bool flat = dev::kFlatAlways<N> || p.flat_eval;
-  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, false, W, flat);
+  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, flat, 16);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -20;
   long long grid = (p.n_items + subs - 1) / subs;
   if (grid > 65535LL * 16) grid = 65535LL * 16;
@@ -60,26 +58,25 @@ int launch_polish_t(const PolishParams& p, cudaStream_t s) {
 #define GHC_P2C_SIZES(X) X(3) X(4) X(5) X(6) X(8) X(10) X(11) X(12) X(16) X(18)
 
 // dispatch of one precision mode over the compiled sizes
-template <typename RS, typename RP, typename RCL, typename RCH>
+template <typename R>
 int launch_mode(const TrackParams& p, cudaStream_t s, int n_sm) {
   using namespace launch_detail;
   if (p.kind == KIND_P2C) {
     switch (p.N) {
 #define CASE(n) \
   case n:       \
-    return launch_track_t<RS, RP, RCL, RCH, n, KIND_P2C>(p, s, n_sm);
+    return launch_track_t<R, n, KIND_P2C>(p, s, n_sm);
       GHC_P2C_SIZES(CASE)
 #undef CASE
       default:
         return -10;
     }
   }
-  if (p.kind == KIND_PH && p.N == 30) return launch_track_t<RS, RP, RCL, RCH, 30, KIND_PH>(p, s, n_sm);
+  if (p.kind == KIND_PH && p.N == 30) return launch_track_t<R, 30, KIND_PH>(p, s, n_sm);
   return -10;
 }
 
 int launch_track_fp64(const TrackParams& p, cudaStream_t s, int n_sm);
 int launch_track_fp32(const TrackParams& p, cudaStream_t s, int n_sm);
-int launch_track_mixed(const TrackParams& p, cudaStream_t s, int n_sm);
 
 }  // namespace ghc

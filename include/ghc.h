@@ -34,7 +34,7 @@ extern "C" {
 
 #define GHC_PREC_FP64 0  /* plain FP64 tracker */
 #define GHC_PREC_FP32 1  /* reference precision (complex FP32) */
-#define GHC_PREC_MIXED 2 /* FP32 predictor, FP32 corrector before t_switch, FP64 after */
+#define GHC_PREC_MIXED 2 /* FP32 tracking to t_switch (early handover on failure), FP64 from there */
 
 #define GHC_STATUS_CONVERGED 0
 #define GHC_STATUS_DIVERGED 1 /* |x|^2 > 1e14 in the corrector ("infinity") */
@@ -110,7 +110,9 @@ typedef struct {
   int32_t max_steps;          /* <= 0: YAML value */
   int32_t max_corr;           /* <= 0: YAML value */
   int32_t incr_steps;         /* <= 0: YAML value */
-  double t_switch;            /* GHC_PREC_MIXED: FP64 corrector for t >= t_switch */
+  double t_switch;            /* GHC_PREC_MIXED: FP32 tracker for t < t_switch (at most 0.95; <= 0: all FP64);
+                                 a path failing 3 steps in a row or diverging goes FP64 at its last
+                                 accepted point; needs d_steps, d_corr, d_t_end, d_dt_end */
   int32_t polish_iters;       /* Newton iterations at t = 1 after tracking (FP64 state only) */
   /* step control; <= 0 selects the reference's value (kernel_HC_Solver_P3P.cu:214) */
   double corr_tol2;           /* corrector success |dx|^2 < corr_tol2 |x|^2 (reference 1e-6) */

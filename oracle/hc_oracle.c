@@ -38,6 +38,13 @@ typedef struct {
   double corr_tol2;  /* corrector success: |dx|^2 < corr_tol2 * |x|^2 */
   double first_tol2; /* reject the step when the first Newton update has |dx|^2 > first_tol2 * |x|^2 */
   double dt_max;     /* upper bound of the step size */
+  /* two-phase mixed precision (the tracker library's GHC_PREC_MIXED, not a reference feature):
+   * the first (float) phase stops a path at t_handover (> 0), after fail_limit (> 0)
+   * consecutive failed steps, or on divergence at its last accepted point; the second
+   * (double) phase resumes every path from endpoints / t_end / dt_end / steps / corr */
+  double t_handover;
+  int32_t fail_limit;
+  int32_t resume;
 } orc_problem;
 
 typedef struct {

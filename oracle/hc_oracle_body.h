@@ -293,6 +293,9 @@ static void SFX(eval_solve)(const orc_problem* pb, const COEFS* cf, const CX* x,
 /*
  * Track one path from t=0 to t=1 (reference HC_solver_<p> body).
  * x_io: in = start point (N values), out = endpoint.
+ * With pb->resume the path starts at out->t_end with step out->dt_end and the
+ * counts out->steps / out->corr; pb->t_handover / fail_limit add the stopping
+ * rules of the first phase of the two-phase mixed-precision tracker.
  */
 static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
   const orc_problem* pb = h->pb;
@@ -304,14 +307,28 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
 
   const int ph = (pb->kind == ORC_PH);
   REAL t0 = 0, t_step = 0, dt = ph ? (REAL)0.01 : (REAL)0.05;
-  int end_zone = 0, nsucc = 0;
+  int end_zone = 0, nsucc = 0, nfail = 0;
   int success = 0, inf = 0;
   int32_t steps = 0, corr = 0;
+  const int handover = pb->t_handover > 0 || pb->fail_limit > 0;
+  const REAL t_hand = (REAL)pb->t_handover;
+  if (pb->resume) {
+    t0 = (REAL)out->t_end;
+    dt = (REAL)out->dt_end;
+    steps = out->steps;
+    corr = out->corr;
+  }
   static const REAL wgt[3] = {(REAL)(1.0 / 6.0), (REAL)(2.0 / 6.0), (REAL)(2.0 / 6.0)};
   static const REAL frac[3] = {(REAL)0.5, (REAL)0.5, (REAL)1.0};
 
-  for (int step = 0; step <= pb->max_steps; ++step) {
+  REAL dt_pre = dt; /* the step without the handover clamp: the next phase resumes with it */
+  for (int step = steps; step <= pb->max_steps; ++step) {
     if (!(t0 < (REAL)1 && (REAL)1 - t0 > (REAL)1e-7)) break;
+    if (pb->t_handover > 0 && t_hand - t0 <= (REAL)1e-6) {
+      if (dt < dt_pre) dt = dt_pre;
+      break;
+    }
+    if (pb->fail_limit > 0 && nfail >= pb->fail_limit) break;
     ++steps;
     /* end-zone step clamp (kernel_HC_Solver_P3P.cu:121-131; PH edge 0.95 at trifocal_2op1p_30x30.cu:163-182) */
     if (!end_zone && FABS((REAL)1 - t0) <= (REAL)0.0500001) end_zone = 1;
@@ -321,6 +338,8 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
       const REAL edge = ph ? FABS((REAL)0.95 - t0) : FABS(((REAL)1 - (REAL)0.05) - t0);
       if (dt > edge) dt = edge;
     }
+    dt_pre = dt;
+    if (pb->t_handover > 0 && dt > t_hand - t0) dt = t_hand - t0;
     t_step = t0;
     const REAL half = (REAL)0.5 * dt;
 
@@ -364,7 +383,13 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
       if (inf || success) break;
       if (it == 0 && (double)sn > pb->first_tol2 * (double)sc) break; /* predictor too far off: reject */
     }
-    if (inf) break;
+    if (inf) {
+      if (handover) { /* hand the last accepted point over */
+        for (int r = 0; r < N; ++r) x[r] = x0[r];
+        t0 = t_step;
+      }
+      break;
+    }
 
     /* step control (kernel_HC_Solver_P3P.cu:230-249) */
     if (!success) {
@@ -372,7 +397,9 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
       for (int r = 0; r < N; ++r) x[r] = sols[r] = x0[r];
       nsucc = 0;
       t0 = t_step;
+      ++nfail;
     } else {
+      nfail = 0;
       ++nsucc;
       for (int r = 0; r < N; ++r) x0[r] = sols[r] = x[r];
       if (nsucc >= pb->incr_steps) {
@@ -424,6 +451,7 @@ int SFX(orc_track)(const orc_problem* pb, int64_t n_items, int32_t paths_per_hyp
   if (pb->kind == ORC_PH && pb->P + 1 > ORC_MMAX) return -3;
   if (pb->Px > 8 || pb->Pt > 8) return -4;
   if (paths_per_hyp <= 0) return -5;
+  if (pb->resume && (!t_end || !dt_end || !steps || !corr)) return -6;
   const int N = pb->N;
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -440,8 +468,16 @@ int SFX(orc_track)(const orc_problem* pb, int64_t n_items, int32_t paths_per_hyp
     h.p_tgt = p_tgt ? (const CX*)(p_tgt + 2 * hy * stride_p) : NULL;
     h.p_diff = p_diff ? (const CX*)(p_diff + 2 * hy * stride_p) : NULL;
     CX x[ORC_NMAX];
-    for (int r = 0; r < N; ++r) x[r] = SFX(c_make)(start_sols[2 * (p * N + r)], start_sols[2 * (p * N + r) + 1]);
     orc_path_out o;
+    if (pb->resume) {
+      for (int r = 0; r < N; ++r) x[r] = SFX(c_make)(endpoints[2 * (i * N + r)], endpoints[2 * (i * N + r) + 1]);
+      o.t_end = t_end[i];
+      o.dt_end = dt_end[i];
+      o.steps = steps[i];
+      o.corr = corr[i];
+    } else {
+      for (int r = 0; r < N; ++r) x[r] = SFX(c_make)(start_sols[2 * (p * N + r)], start_sols[2 * (p * N + r) + 1]);
+    }
     SFX(track_path)(&h, x, &o);
     for (int r = 0; r < N; ++r) {
       endpoints[2 * (i * N + r)] = x[r].re;

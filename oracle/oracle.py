@@ -178,7 +178,8 @@ class _Prob(ctypes.Structure):
                 ("max_steps", ctypes.c_int32), ("max_corr", ctypes.c_int32),
                 ("incr_steps", ctypes.c_int32), ("polish_iters", ctypes.c_int32),
                 ("hx_idx", ctypes.c_void_p), ("ht_idx", ctypes.c_void_p), ("corr_tol2", ctypes.c_double),
-                ("first_tol2", ctypes.c_double), ("dt_max", ctypes.c_double)]
+                ("first_tol2", ctypes.c_double), ("dt_max", ctypes.c_double),
+                ("t_handover", ctypes.c_double), ("fail_limit", ctypes.c_int32), ("resume", ctypes.c_int32)]
 
 # step control of the reference (kernel_HC_Solver_P3P.cu:214, no contraction test, no dt cap)
 REFERENCE_STEP = dict(corr_tol2=1e-6, first_tol2=float("inf"), dt_max=float("inf"))
@@ -223,14 +224,40 @@ def _prob_struct(pb, polish_iters, max_steps=None, max_corr=None, incr=None, ste
     return s
 
 
+# the tracker library's two-phase mixed precision (csrc/tracker.cu): float tracking to
+# min(t_switch, 0.95), a path handed over after 3 failed steps in a row or on divergence
+MIXED_FAIL_LIMIT = 3
+MIXED_MAX_SWITCH = 0.95
+MIXED_F32_TOL2 = 1e-7  # the float phase's corrector tolerance floor
+
+
 def track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precision="d",
-          polish_iters=0, nthreads=0, max_steps=None, max_corr=None, incr=None, step=None):
+          polish_iters=0, nthreads=0, max_steps=None, max_corr=None, incr=None, step=None, t_switch=0.9):
     """Track all start paths for H hypotheses.
 
     P2C: hx [H, (M+1)(K+1)], ht [H, (M+1)K] complex.
     PH:  p_start [P+1], p_target [H, P+1] complex.
+    precision "d", "f", or "mixed": float tracking to t_switch (with handover), then
+    double resumed from each path's last accepted point, as the tracker library does.
     Returns a dict of numpy arrays (endpoints [H*paths, N], flags, counters).
     """
+    kw = dict(hx=hx, ht=ht, p_start=p_start, p_target=p_target, nthreads=nthreads, max_steps=max_steps,
+              max_corr=max_corr, incr=incr, step=step)
+    if precision != "mixed":
+        return _track(pb, start_sols, precision=precision, polish_iters=polish_iters, **kw)
+    if not t_switch > 0:
+        return _track(pb, start_sols, precision="d", polish_iters=polish_iters, **kw)
+    st = dict(REFERENCE_STEP)
+    st.update(step or {})
+    st["corr_tol2"] = max(st["corr_tol2"], MIXED_F32_TOL2)
+    first = _track(pb, start_sols, precision="f", polish_iters=0,
+                   handover=(min(t_switch, MIXED_MAX_SWITCH), MIXED_FAIL_LIMIT), **dict(kw, step=st))
+    return _track(pb, start_sols, precision="d", polish_iters=polish_iters, resume=first, **kw)
+
+
+def _track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precision="d",
+           polish_iters=0, nthreads=0, max_steps=None, max_corr=None, incr=None, step=None, handover=None,
+           resume=None):
     rt = np.float64 if precision == "d" else np.float32
     fn = lib().orc_track_d if precision == "d" else lib().orc_track_f
     start_sols = np.asarray(start_sols)
@@ -259,6 +286,13 @@ def track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precisi
                steps=np.zeros(n, np.int32), corr=np.zeros(n, np.int32), t_end=np.zeros(n),
                dt_end=np.zeros(n), resid=np.zeros(n))
     s = _prob_struct(pb, polish_iters, max_steps, max_corr, incr, step)
+    if handover is not None:
+        s.t_handover, s.fail_limit = handover
+    if resume is not None:
+        s.resume = 1
+        ep[...] = resume["endpoints_raw"].astype(rt)
+        for k in ("steps", "corr", "t_end", "dt_end"):
+            out[k][:] = resume[k]
     P = ctypes.c_void_p
 
     def ptr(a):

@@ -2,7 +2,8 @@
 
 FP64 and FP32 modes follow the oracle's operation order, so endpoints, flags
 and step/iteration counters must be identical (compared as values).  Mixed
-precision is checked by recall of the FP64 real endpoints after FP64 polish.
+precision (FP32 to t_switch with handover, then FP64) is compared the same way
+with the oracle's two-phase run, and by recall of the FP64 real endpoints.
 """
 import os
 
@@ -108,6 +109,36 @@ def test_fp32_bit_exact_vs_oracle(name):
     compare(ws, r)
 
 
+@pytest.mark.parametrize("name,robust,t_switch", [("P3P", False, 0.9), ("generalized_3views_4pts", False, 0.9),
+                                                  ("generalized_3views_4pts", True, 0.5),
+                                                  ("uncalibrated_trifocal_rel_pos_CY", False, 0.9),
+                                                  ("5pt_rel_pos_alg_form_quat", False, 0.7),
+                                                  ("trifocal_2op1p_30x30", False, 0.9)])
+def test_mixed_bit_exact_vs_oracle(name, robust, t_switch):
+    """Both phases, the handover state and the FP64 resume match the oracle bit for bit."""
+    pb, ob, tg = inputs(name, n_hyp=2, seed=3)
+    kw = ROBUST if robust else {}
+    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=2, t_switch=t_switch, **kw)
+    r = O.track(ob, ob.start_sols, precision="mixed", t_switch=t_switch, polish_iters=2, nthreads=NCPU,
+                **oargs, **kw)
+    compare(ws, r)
+    conv = r["conv"] == 1
+    assert np.array_equal(ws.resid.cpu().numpy()[conv], r["resid"][conv])
+
+
+def test_mixed_handover_happens():
+    """The FP32 phase stops every path by t_switch, and the FP64 phase carries its step
+    counts on (a path's steps are those of both phases, under one step cap)."""
+    pb, ob, tg = inputs("generalized_3views_4pts")
+    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_MIXED, t_switch=0.5, max_steps=6)
+    r_mixed = O.track(ob, ob.start_sols, precision="mixed", t_switch=0.5, max_steps=6, nthreads=NCPU, **oargs)
+    compare(ws, r_mixed)
+    first = O._track(ob, ob.start_sols.astype(np.complex64), precision="f", max_steps=6, handover=(0.5, 3),
+                     hx=oargs["hx"].astype(np.complex64), ht=oargs["ht"].astype(np.complex64))
+    assert (first["t_end"] <= 0.5 + 1e-6).all()
+    assert (ws.steps.cpu().numpy() >= first["steps"]).all()
+
+
 @pytest.mark.parametrize("name", ["P3P", "generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY"])
 def test_batched_hypotheses_equal_single_runs(name):
     pb, ob, tg = inputs(name, n_hyp=3, seed=5)
@@ -143,12 +174,12 @@ def real_targets(ob, n_hyp, seed):
 @pytest.mark.parametrize("name", ["generalized_3views_4pts", "5pt_rel_pos_alg_form_quat",
                                   "uncalibrated_trifocal_rel_pos_CY"])
 def test_mixed_precision_recall(name):
-    """FP32 predictor + FP64 corrector, both runs with path-jump-free step control:
+    """FP32 tracking to t = 0.9 then FP64, both runs with path-jump-free step control:
     >= 99.5% of the FP64 run's real endpoints are found by the mixed run within 1e-8."""
     pb, ob = ghc.Problem(name), O.Problem(name)
     tg = real_targets(ob, 2, 9)
     w64, _ = run_gpu(pb, ob, tg, ghc.PREC_FP64, polish=3, **ROBUST)
-    wmx, _ = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=3, t_switch=0.0, **ROBUST)
+    wmx, _ = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=3, t_switch=0.9, **ROBUST)
     e64, emx = to_cx(w64.endpoints), to_cx(wmx.endpoints)
     c64, cmx = w64.conv.cpu().numpy() == 1, wmx.conv.cpu().numpy() == 1
     r64 = w64.resid.cpu().numpy()

@@ -157,3 +157,21 @@ def test_p3p_known_answer():
     r = O.track(pb, pb.start_sols, hx=hx, ht=ht, polish_iters=3)
     assert r["conv"].all() and not r["inf"].any()
     assert np.nanmax(r["resid"]) < 1e-10
+
+
+def test_oracle_two_phase_mixed():
+    """The oracle's two-phase mixed run: the float phase stops every path by t_switch (handover),
+    the double phase resumes it to t = 1 under the same step cap; t_switch <= 0 is plain double."""
+    pb = O.Problem("generalized_3views_4pts")
+    hx, ht = coefs(pb)
+    first = O._track(pb, pb.start_sols.astype(np.complex64), precision="f", handover=(0.6, 3),
+                     hx=hx.astype(np.complex64), ht=ht.astype(np.complex64), nthreads=4)
+    assert (first["t_end"] <= 0.6 + 1e-6).all() and (first["conv"] == 0).all()
+    mixed = O.track(pb, pb.start_sols, hx=hx, ht=ht, precision="mixed", t_switch=0.6, polish_iters=3, nthreads=4)
+    assert (mixed["steps"] >= first["steps"]).all() and (mixed["steps"] <= pb.max_steps + 1).all()
+    assert mixed["conv"].mean() > 0.99
+    conv = mixed["conv"] == 1
+    assert np.median(mixed["resid"][conv]) < 1e-10
+    plain = O.track(pb, pb.start_sols, hx=hx, ht=ht, polish_iters=3, nthreads=4)
+    zero = O.track(pb, pb.start_sols, hx=hx, ht=ht, precision="mixed", t_switch=0.0, polish_iters=3, nthreads=4)
+    assert np.array_equal(plain["endpoints"], zero["endpoints"])

@@ -309,8 +309,8 @@ int ghc_problem_get_info(const ghc_problem* h, ghc_problem_info* info) {
   info->max_steps = pb.max_steps;
   info->max_corr = pb.max_corr;
   info->incr_steps = pb.incr;
-  info->n_hx_terms = (int)pb.hx_terms.size();
-  info->n_ht_terms = (int)pb.ht_terms.size();
+  info->n_hx_terms = (int)pb.hx_off.back();
+  info->n_ht_terms = (int)pb.ht_off.back();
   info->has_p2c_terms = pb.has_terms ? 1 : 0;
   info->subwarp = track_subwarp_width(pb.N);
   return GHC_OK;

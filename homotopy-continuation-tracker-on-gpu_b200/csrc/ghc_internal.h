@@ -7,7 +7,8 @@
 //
 // The device never walks the raw tables.  The host compiles them once into
 // "terms": one 64-bit word per non-padding monomial term, grouped by Jacobian
-// entry (row, col) for H_x and by row for H / H_t, with CSR offsets.
+// entry (row, col) for H_x and by row for H / H_t, with CSR offsets; the words
+// are stored row-interleaved (term k of row r at k * N + r).
 #pragma once
 #include <cstdint>
 

@@ -197,6 +197,21 @@ int compile_tables(const std::vector<int32_t>& hx, const std::vector<int32_t>& h
     }
   }
   ht_off[N] = (uint16_t)ht_terms.size();
+  // Row-interleaved storage: term k of row r at k * N + r, rows padded with zero
+  // words to the longest row, so the lanes of a sub-warp (one row each) read
+  // consecutive words of shared memory.  The CSR offsets keep their meaning:
+  // term j of row r (hx_off[r N] <= j < hx_off[(r+1) N]) sits at (j - hx_off[r N]) N + r.
+  auto interleave = [&](std::vector<uint64_t>& terms, const std::vector<uint16_t>& off, int per_row) {
+    int longest = 0;
+    for (int r = 0; r < N; ++r) longest = std::max(longest, off[(size_t)(r + 1) * per_row] - off[(size_t)r * per_row]);
+    std::vector<uint64_t> out((size_t)longest * N, 0);
+    for (int r = 0; r < N; ++r)
+      for (int k = off[(size_t)r * per_row]; k < off[(size_t)(r + 1) * per_row]; ++k)
+        out[(size_t)(k - off[(size_t)r * per_row]) * N + r] = terms[k];
+    terms.swap(out);
+  };
+  interleave(hx_terms, hx_off, N);
+  interleave(ht_terms, ht_off, 1);
   if (hx_terms.size() > 60000 || ht_terms.size() > 60000) {
     set_error("too many terms");
     return GHC_ERR_LIMIT;

@@ -30,9 +30,9 @@ int track_subwarp_width(int N) {
   return 32;
 }
 
-constexpr int kMixedFailLimit = 3;
+constexpr int kMixedFailLimit = 2;
 constexpr double kMixedMaxSwitch = 0.95;
-constexpr double kMixedF32Tol2 = 1e-7;
+constexpr double kMixedF32Tol2 = 1e-9;
 
 int launch_track(const TrackParams& p, int precision, double t_switch, void* stream, int n_sm) {
   cudaStream_t s = (cudaStream_t)stream;

@@ -192,9 +192,9 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
     for (int i = 0; i < N; ++i) {
       cx<R> acc = mk(R(0), R(0));
       if (live) {
-        const int j0 = tb.hx_off[r * N + i], j1 = tb.hx_off[r * N + i + 1];
+        const int base = tb.hx_off[r * N], j0 = tb.hx_off[r * N + i], j1 = tb.hx_off[r * N + i + 1];
         for (int j = j0; j < j1; ++j) {
-          const uint64_t w = tb.hx_terms[j];
+          const uint64_t w = tb.hx_terms[(j - base) * N + r];
           acc = acc_term(acc, term_coef_value<R, KIND>(w, ca), w, xs);
         }
       }
@@ -202,11 +202,11 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
     }
   } else {
     if (live) {
-      const int j0 = tb.hx_off[r * N], j1 = tb.hx_off[r * N + N];
+      const int len = tb.hx_off[r * N + N] - tb.hx_off[r * N];
       int cur = -1;
       cx<R> acc = mk(R(0), R(0));
-      for (int j = j0; j < j1; ++j) {
-        const uint64_t w = tb.hx_terms[j];
+      for (int k = 0; k < len; ++k) {
+        const uint64_t w = tb.hx_terms[k * N + r];
         const int i = term_col(w);
         if (i != cur) {
           if (cur >= 0) *slot(cur) = acc;
@@ -222,9 +222,9 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
   }
   cx<R> h = mk(R(0), R(0));
   if (live) {
-    const int j0 = tb.ht_off[r], j1 = tb.ht_off[r + 1];
-    for (int j = j0; j < j1; ++j) {
-      const uint64_t w = tb.ht_terms[j];
+    const int len = tb.ht_off[r + 1] - tb.ht_off[r];
+    for (int k = 0; k < len; ++k) {
+      const uint64_t w = tb.ht_terms[k * N + r];
       cx<R> p;
       if (KIND == KIND_P2C) {
         p = c_scale((R)term_scale(w), which ? cb[term_coef(w)] : ca[term_coef(w)]);
@@ -267,8 +267,9 @@ __device__ __forceinline__ void static_for(F&& f) {
 // Partial-pivot LU + back substitution, one row per lane, rows in registers.
 // The pivot is found by an integer max butterfly over the sub-warp.  A
 // zero pivot skips that column's elimination and leaves a non-finite
-// solution, as in the reference.  Solution lands in sol[0..N); sx holds
-// N+1 entries (pivot row + its right-hand side).
+// solution, as in the reference.  Solution lands in sol[0..N); sx holds two
+// pivot-row buffers of N+1 entries (row + right-hand side), used by
+// alternate columns so that one __syncwarp per column suffices.
 //
 // Two code shapes with the same operations in the same order:
 //   LU_UNROLLED  every column unrolled at compile time (template recursion, so
@@ -292,6 +293,9 @@ __device__ __forceinline__ int pivot_search(cx<R> a, bool live, int pos, int i) 
   return 31 - (int)(best & 31u);
 }
 
+#ifndef GHC_LU_SELECT
+#define GHC_LU_SELECT 0
+#endif
 template <typename R, int N, int W>
 __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
   const bool live = l < N;
@@ -299,6 +303,7 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
   cx<R> myrcp = mk(R(0), R(0));
   static_for<0, N>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
+    cx<R>* px = sx + (i & 1) * (N + 1);
     const int bp = pivot_search<R, W>(A[i], live, pos, i);
     const bool is_piv = live && (pos == bp);
     if (live) {
@@ -306,23 +311,37 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
       else if (pos == i) pos = bp;
     }
     if (is_piv) {
-      static_for<i, N>([&](auto jc) { sx[decltype(jc)::value] = A[decltype(jc)::value]; });
-      sx[N] = b;
+      static_for<i, N>([&](auto jc) { px[decltype(jc)::value] = A[decltype(jc)::value]; });
+      px[N] = b;
     }
     __syncwarp(kFull);
-    const cx<R> p_i = sx[i];
+    const cx<R> p_i = px[i];
     const bool zero = (fabs(p_i.re) + fabs(p_i.im) == R(0));
     const cx<R> rc = c_rcp(zero ? mk(R(0), R(0)) : p_i);
     if (is_piv) myrcp = rc;
-    if (live && pos > i && !zero) {
+    // rows below the pivot take the update, the others keep their values
+    const bool upd = live && pos > i && !zero;
+#if GHC_LU_SELECT
+    // by selects: no branch, so the next column's pivot search can overlap these updates
+    const cx<R> m = c_mul(A[i], rc);
+    A[i] = upd ? m : A[i];
+    static_for<i + 1, N>([&](auto jc) {
+      constexpr int j = decltype(jc)::value;
+      const cx<R> v = c_fnma(m, px[j], A[j]);
+      A[j] = upd ? v : A[j];
+    });
+    const cx<R> vb = c_fnma(m, px[N], b);
+    b = upd ? vb : b;
+#else
+    if (upd) {
       A[i] = c_mul(A[i], rc);
       static_for<i + 1, N>([&](auto jc) {
         constexpr int j = decltype(jc)::value;
-        A[j] = c_fnma(A[i], sx[j], A[j]);
+        A[j] = c_fnma(A[i], px[j], A[j]);
       });
-      b = c_fnma(A[i], sx[N], b);
+      b = c_fnma(A[i], px[N], b);
     }
-    __syncwarp(kFull);
+#endif
   });
   static_for<0, N>([&](auto ic) {
     constexpr int i = N - 1 - decltype(ic)::value;
@@ -410,7 +429,7 @@ struct SubMem {
   unsigned char* coefA;  // c_k(t)   or p(t)     [Mc]
   unsigned char* coefB;  // c'_k(t)  or p1 - p0  [Mc]
   unsigned char* xs;     // track [N+1]
-  unsigned char* sx;     // pivot row + rhs [N+1]
+  unsigned char* sx;     // two pivot rows + rhs [2][N+1]
   unsigned char* sol;    // solution [N]
   unsigned char* state;  // per lane: RK base point x0 [W], RK accumulator [W]
   unsigned char* scr;    // H_x row scratch [N][W], null unless the evaluation is flat
@@ -451,10 +470,10 @@ __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t
 __host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
   return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(N * N + 1 + N + 1));
 }
-// per sub-warp, in complex values of esz bytes: coefficient buffers [2 Mc], track and
-// pivot row [2 (N+1)], solution [N], lane state [2 W], scratch row [N W] when flat
+// per sub-warp, in complex values of esz bytes: coefficient buffers [2 Mc], track [N+1],
+// two pivot rows [2 (N+1)], solution [N], lane state [2 W], scratch row [N W] when flat
 __host__ __device__ inline size_t sub_bytes(int N, int Mc, int W, bool flat, int esz) {
-  return align16((size_t)esz * (2 * (size_t)Mc + 2 * (N + 1) + N + 2 * W + (flat ? N * W : 0)));
+  return align16((size_t)esz * (2 * (size_t)Mc + 3 * (N + 1) + N + 2 * W + (flat ? N * W : 0)));
 }
 template <typename R>
 __device__ __forceinline__ SubMem sub_layout(unsigned char* base, int N, int Mc, int W, bool flat) {
@@ -464,7 +483,7 @@ __device__ __forceinline__ SubMem sub_layout(unsigned char* base, int N, int Mc,
   sm.coefB = base + e * (size_t)Mc;
   sm.xs = base + 2 * e * (size_t)Mc;
   sm.sx = sm.xs + e * (N + 1);
-  sm.sol = sm.sx + e * (N + 1);
+  sm.sol = sm.sx + 2 * e * (N + 1);
   sm.state = sm.sol + e * N;
   sm.scr = flat ? sm.state + 2 * e * W : nullptr;
   return sm;
@@ -490,10 +509,10 @@ __device__ __forceinline__ cx<R> load_cx(const void* base, bool f64, long long i
 
 // CTAs per SM the tracker asks the register allocator for: the row of H_x (N
 // complex values) dominates the registers, so small systems afford more.
-// Measured on B200: FP64 N = 3 best at 8, N = 6 and N = 12 at 4.
+// Measured on B200: FP64 N = 3 best at 6 (64 registers spill), N = 6 and N = 12 at 4.
 template <int N, typename R>
 constexpr int track_min_blocks() {
-  return sizeof(R) == 8 ? (N <= 4 ? 8 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
+  return sizeof(R) == 8 ? (N <= 4 ? 6 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
                         : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 3);
 }
 
@@ -719,7 +738,11 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R)) track_kernel(const TrackP
         if (p.status) p.status[item] = conv ? ST_CONVERGED : (inf ? ST_DIVERGED : ST_STEP_CAP);
         if (p.steps) p.steps[item] = step;
         if (p.corr) p.corr[item] = ncorr;
-        if (p.t_end) p.t_end[item] = (double)t0;
+        // a path handed over at the boundary resumes at exactly t_handover, not at its float t
+        // (a float t just short of the boundary would put the next step just short of the end
+        // zone, where the edge clamp shrinks dt to the gap)
+        const bool boundary = p.t_handover > 0.0 && !inf && f_sub(t_hand, t0) <= R(1e-6);
+        if (p.t_end) p.t_end[item] = boundary ? p.t_handover : (double)t0;
         if (p.dt_end) p.dt_end[item] = (double)dt;
       }
     }

@@ -111,7 +111,7 @@ typedef struct {
   int32_t max_corr;           /* <= 0: YAML value */
   int32_t incr_steps;         /* <= 0: YAML value */
   double t_switch;            /* GHC_PREC_MIXED: FP32 tracker for t < t_switch (at most 0.95; <= 0: all FP64);
-                                 a path failing 3 steps in a row or diverging goes FP64 at its last
+                                 a path failing 2 steps in a row or diverging goes FP64 at its last
                                  accepted point; needs d_steps, d_corr, d_t_end, d_dt_end */
   int32_t polish_iters;       /* Newton iterations at t = 1 after tracking (FP64 state only) */
   /* step control; <= 0 selects the reference's value (kernel_HC_Solver_P3P.cu:214) */

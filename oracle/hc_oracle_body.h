@@ -416,7 +416,8 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
   out->status = conv ? ORC_CONVERGED : (inf ? ORC_DIVERGED : ORC_STEP_CAP);
   out->steps = steps;
   out->corr = corr;
-  out->t_end = (double)t0;
+  /* handed over at the boundary: resume at exactly t_handover (the tracker library does the same) */
+  out->t_end = (pb->t_handover > 0 && !inf && t_hand - t0 <= (REAL)1e-6) ? pb->t_handover : (double)t0;
   out->dt_end = (double)dt;
 
   /* optional Newton polish at t = 1 of converged paths, then the residual |H(x,1)| */

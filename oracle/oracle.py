@@ -225,10 +225,10 @@ def _prob_struct(pb, polish_iters, max_steps=None, max_corr=None, incr=None, ste
 
 
 # the tracker library's two-phase mixed precision (csrc/tracker.cu): float tracking to
-# min(t_switch, 0.95), a path handed over after 3 failed steps in a row or on divergence
-MIXED_FAIL_LIMIT = 3
+# min(t_switch, 0.95), a path handed over after 2 failed steps in a row or on divergence
+MIXED_FAIL_LIMIT = 2
 MIXED_MAX_SWITCH = 0.95
-MIXED_F32_TOL2 = 1e-7  # the float phase's corrector tolerance floor
+MIXED_F32_TOL2 = 1e-9  # the float phase's corrector tolerance floor
 
 
 def track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precision="d",

@@ -38,6 +38,30 @@ UNIT = "hypotheses/s"
 ROBUST = dict(corr_tol2=1e-12, first_tol2=1e-2, dt_max=0.05)
 
 
+# ----------------------------------------------------------------------------------------------
+# ranks: hypothesis shards, max-over-ranks time, whole-job rate (tests/test_multi_rank.py)
+# ----------------------------------------------------------------------------------------------
+
+def rank_seed(seed, rank):
+    """Scene seed of a rank's shard: every rank tracks its own, distinct hypotheses."""
+    return seed * 7919 + rank
+
+
+def max_over_ranks(dist, v, device):
+    """The slowest rank's value (the job's elapsed time); plain v on one process."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, hyp_per_rank, steps, total_ms):
+    """Hypotheses of all ranks per second of the slowest rank (weak scaling)."""
+    return world * hyp_per_rank * steps / (total_ms * 1e-3)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -225,18 +249,11 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     H = args.hyp
     pb = ghc.Problem(PROBLEM)
     s_host, _ = pb.params()
     starts = pb.start_sols()
-    tg, _truth = scenes.generalized_3views_4pts(H, seed=args.seed * 7919 + rank)
+    tg, _truth = scenes.generalized_3views_4pts(H, seed=rank_seed(args.seed, rank))
     d_start = cx(s_host)
     d_tg = cx(tg)
     d_sols = cx(starts)
@@ -274,9 +291,9 @@ def main():
             step_ms.append(e0.elapsed_time(e1))
             kern_ms.append(k0.elapsed_time(k1))
         barrier()
-    total_ms = max_over_ranks(sum(step_ms))
+    total_ms = max_over_ranks(dist, sum(step_ms), dev)
     n_steps = args.steps
-    value = world * H * n_steps / (total_ms * 1e-3)
+    value = whole_job_rate(world, H, n_steps, total_ms)
 
     # ---------------- results of the timed batch (last step)
     steps = ws.steps.cpu().numpy()

@@ -496,6 +496,28 @@ int ghc_count_results(int32_t N, int32_t paths, const double* z, const uint8_t* 
   return GHC_OK;
 }
 
+int ghc_count_results_device(int32_t N, int32_t paths, int64_t n_hyp, const double* d_endpoints,
+                             const uint8_t* d_conv, const uint8_t* d_inf, double imag_tol, double dup_tol,
+                             ghc_counts* d_counts, uint8_t* d_class, void* stream) {
+  if (N < 1 || N > kMaxN || paths < 0 || n_hyp < 0) {
+    set_error("bad size");
+    return GHC_ERR_ARG;
+  }
+  if (n_hyp == 0 || paths == 0) return GHC_OK;
+  if (!d_endpoints || !d_conv || !d_inf || !d_counts) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  if (paths > 200000) {
+    set_error("more than 200,000 paths per hypothesis");
+    return GHC_ERR_RANGE;
+  }
+  if (launch_results(N, paths, n_hyp, d_endpoints, d_conv, d_inf, imag_tol, dup_tol, (int*)d_counts, d_class,
+                     stream))
+    return cuda_fail("result counts");
+  return GHC_OK;
+}
+
 double ghc_kernel_HC_Solver_P2C(const ghc_problem* pb, void* stream, int max_steps, int max_corr, int incr,
                                 float** d_startSols_array, float** d_Track_array, const int* d_Hx_idx,
                                 const int* d_Ht_idx, const float* d_phc_coeffs_Hx, const float* d_phc_coeffs_Ht,

@@ -170,5 +170,9 @@ int launch_track(const TrackParams& p, int precision, double t_switch, void* str
 int launch_polish(const PolishParams& p, void* stream);
 int launch_p2c(const P2CParams& p, void* stream);
 int track_subwarp_width(int N);
+// results.cu: per-hypothesis counts (int[4] per hypothesis) and class bytes on the device
+size_t results_smem_bytes(int paths);
+int launch_results(int N, int paths, long long n_hyp, const double* z, const uint8_t* conv, const uint8_t* inf,
+                   double imag_tol, double dup_tol, int* counts, uint8_t* cls, void* stream);
 
 }  // namespace ghc

@@ -74,6 +74,8 @@ ghc_track = _sig("ghc_track", ctypes.c_int, [_P, ctypes.POINTER(TrackArgs), _P])
 ghc_track_noalloc = _sig("ghc_track_noalloc", ctypes.c_int, [_P, ctypes.POINTER(TrackArgs), _P])
 ghc_count_results = _sig("ghc_count_results", ctypes.c_int,
                          [_I32, _I32, _P, _P, _P, ctypes.c_double, ctypes.c_double, ctypes.POINTER(Counts)])
+ghc_count_results_device = _sig("ghc_count_results_device", ctypes.c_int,
+                                [_I32, _I32, _I64, _P, _P, _P, ctypes.c_double, ctypes.c_double, _P, _P, _P])
 ghc_solve_host = _sig("ghc_solve_host", ctypes.c_int,
                       [_P, _I32, _I64, _P, ctypes.c_double, _I32, _P, _P, _P, _P, _P, _P])
 _DROPIN_P2C = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P]
@@ -249,6 +251,24 @@ def count_results(endpoints, conv, inf, imag_tol=1e-4, dup_tol=1e-4):
     _check(ghc_count_results(z.shape[1], z.shape[0], z.ctypes.data, c.ctypes.data, i.ctypes.data, imag_tol, dup_tol,
                              ctypes.byref(out)), "ghc_count_results")
     return dict(converged=out.converged, real=out.real, infinity=out.infinity, unique=out.unique)
+
+
+def count_results_device(ws, N, imag_tol=1e-4, dup_tol=1e-4, want_class=False):
+    """Counts of every hypothesis of a workspace, on the device (torch's current stream).
+
+    Returns (counts int32 tensor [n_hyp, 4] = converged, real, infinity, unique;
+    class uint8 tensor [n_hyp * paths] or None): bit 0 converged, bit 1 real,
+    bit 2 counted as unique.  Needs FP64 endpoints (FP64 or mixed workspace).
+    """
+    import torch
+    if ws.endpoints.dtype != torch.float64:
+        raise GhcError("count_results_device needs FP64 endpoints")
+    counts = torch.zeros((ws.n_hyp, 4), dtype=torch.int32, device=ws.endpoints.device)
+    cls = torch.zeros(ws.n_hyp * ws.paths, dtype=torch.uint8, device=ws.endpoints.device) if want_class else None
+    _check(ghc_count_results_device(N, ws.paths, ws.n_hyp, ws.endpoints.data_ptr(), ws.conv.data_ptr(),
+                                    ws.inf.data_ptr(), imag_tol, dup_tol, counts.data_ptr(),
+                                    None if cls is None else cls.data_ptr(), _stream()), "ghc_count_results_device")
+    return counts, cls
 
 
 def solve_host(pb, precision=PREC_FP64, targets=None, t_switch=0.9, polish_iters=0):

@@ -167,6 +167,20 @@ int ghc_count_results(int32_t N, int32_t paths, const double* h_endpoints, const
                       const uint8_t* h_inf, double imag_tol, double dup_tol, ghc_counts* out);
 
 /* ---------------------------------------------------------------------------
+ * Result counts of every hypothesis of a batch on the device (asynchronous on
+ * `stream`), with the rules of ghc_count_results -- the batched, on-device form
+ * of Evaluations::Evaluate_GPUHC_Sols / Find_Unique_Sols
+ * (GPU-HC/magmaHC/Evaluations.cpp:88-110, 127-176).
+ * d_endpoints [n_hyp][paths][N] complex double (the tracker's layout);
+ * d_conv, d_inf [n_hyp][paths]; d_counts [n_hyp] out; d_class [n_hyp][paths] out
+ * (optional): bit 0 converged, bit 1 real, bit 2 counted as unique.
+ * paths up to 200,000.
+ * ------------------------------------------------------------------------- */
+int ghc_count_results_device(int32_t N, int32_t paths, int64_t n_hyp, const double* d_endpoints,
+                             const uint8_t* d_conv, const uint8_t* d_inf, double imag_tol, double dup_tol,
+                             ghc_counts* d_counts, uint8_t* d_class, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Drop-in launch wrappers with the reference kernel ABI
  * (GPU-HC/magmaHC/gpu-kernels/magmaHC-kernels.hpp, e.g. kernel_HC_Solver_P3P.cu:267-282
  * and kernel_HC_Solver_trifocal_2op1p_30x30.cu:413-427).  magma_queue_t becomes a

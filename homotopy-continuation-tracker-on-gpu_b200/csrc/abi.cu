@@ -160,7 +160,7 @@ int dropin_tables(Problem& pb, const int* d_hx, const int* d_ht, TrackParams& p,
   p.ht_off = (const uint16_t*)d;
   p.n_hx_terms = (int)hxt.size();
   p.n_ht_terms = (int)htt.size();
-  p.flat_eval = flat_eval_pays(hxo.data(), pb.N);
+  p.flat_eval = flat_eval_pays(hxo.data(), pb.N);  // the caller's own tables: their own walk
   return GHC_OK;
 }
 
@@ -190,6 +190,7 @@ double dropin(const ghc_problem* h, void* stream, int max_steps, int max_corr, i
   if ((rc = regular_base(d_start_arr, n, pb.N, &start_base)) || (rc = regular_base(d_track_arr, n, pb.N, &track_base)))
     return rc;
   TrackParams p = base_params(pb);
+  apply_tuning(pb, fp32 ? PREC_FP32 : PREC_FP64, p);
   TmpFree tmp;
   if ((rc = dropin_tables(pb, d_hx, d_ht, p, tmp.v))) return rc;
   p.max_steps = max_steps;
@@ -396,6 +397,7 @@ int ghc_track(const ghc_problem* h, const ghc_track_args* a, void* stream) {
   int rc = ensure_device(pb);
   if (rc) return rc;
   TrackParams p = base_params(pb);
+  apply_tuning(pb, a->precision, p);
   if (a->max_steps > 0) p.max_steps = a->max_steps;
   if (a->max_corr > 0) p.max_corr = a->max_corr;
   if (a->incr_steps > 0) p.incr = a->incr_steps;
@@ -493,6 +495,99 @@ int ghc_count_results(int32_t N, int32_t paths, const double* z, const uint8_t* 
     else skip = dup;
   }
   *out = c;
+  return GHC_OK;
+}
+
+int ghc_set_tuning(ghc_problem* h, int32_t precision, int32_t variant, int32_t flat) {
+  if (!h || (variant != 0 && variant != 1) || flat < -1 || flat > 1 ||
+      (precision != GHC_PREC_FP64 && precision != GHC_PREC_FP32 && precision != GHC_PREC_MIXED)) {
+    set_error("bad tuning argument");
+    return GHC_ERR_ARG;
+  }
+  Problem& pb = h->pb;
+  if (precision != GHC_PREC_FP32) {
+    pb.tune_variant[0] = variant;
+    pb.tune_flat[0] = flat;
+  }
+  if (precision != GHC_PREC_FP64) {
+    pb.tune_variant[1] = variant;
+    pb.tune_flat[1] = flat;
+  }
+  return GHC_OK;
+}
+
+int ghc_get_tuning(const ghc_problem* h, int32_t precision, int32_t* variant, int32_t* flat) {
+  if (!h || !variant || !flat || (precision != GHC_PREC_FP64 && precision != GHC_PREC_FP32)) {
+    set_error("bad tuning argument");
+    return GHC_ERR_ARG;
+  }
+  const int k = precision == GHC_PREC_FP32 ? 1 : 0;
+  *variant = h->pb.tune_variant[k];
+  *flat = h->pb.tune_flat[k];
+  return GHC_OK;
+}
+
+int ghc_autotune(ghc_problem* h, const ghc_track_args* a, void* stream, ghc_tune_choice* best) {
+  if (!h || !a || !best) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  Problem& pb = h->pb;
+  const int prec = a->precision;
+  if (prec != GHC_PREC_FP64 && prec != GHC_PREC_FP32 && prec != GHC_PREC_MIXED) {
+    set_error("unknown precision mode");
+    return GHC_ERR_ARG;
+  }
+  std::vector<std::pair<int, int>> cand;
+  for (int v = 0; v < 2; ++v) {
+    if (pb.N > 16) {
+      cand.push_back({v, 1});
+    } else {
+      cand.push_back({v, 1});
+      cand.push_back({v, 0});
+    }
+  }
+  const int keep_v[2] = {pb.tune_variant[0], pb.tune_variant[1]};
+  const int keep_f[2] = {pb.tune_flat[0], pb.tune_flat[1]};
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return cuda_fail("autotune events");
+  double best_ms = HUGE_VAL;
+  int rc = GHC_OK;
+  std::pair<int, int> win = cand[0];
+  for (const auto& c : cand) {
+    ghc_set_tuning(h, prec, c.first, c.second);
+    for (int rep = 0; rep < 2 && !rc; ++rep) {  // the first run warms up (kernel attributes, caches)
+      cudaEventRecord(e0, st);
+      rc = ghc_track(h, a, stream);
+      cudaEventRecord(e1, st);
+    }
+    if (rc) break;
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = cuda_fail("autotune run");
+      break;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      win = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) {  // leave the handle as it was
+    pb.tune_variant[0] = keep_v[0];
+    pb.tune_variant[1] = keep_v[1];
+    pb.tune_flat[0] = keep_f[0];
+    pb.tune_flat[1] = keep_f[1];
+    return rc;
+  }
+  ghc_set_tuning(h, prec, win.first, win.second);
+  best->variant = win.first;
+  best->flat = win.second;
+  best->ms = best_ms;
+  best->candidates = (int)cand.size();
   return GHC_OK;
 }
 

@@ -71,7 +71,9 @@ struct TrackParams {
   int kind, N, P, M, K;
   int max_steps, max_corr, incr;
   int n_hx_terms, n_ht_terms;
-  int flat_eval;              // flat_eval_pays() of the tables
+  int flat_eval;              // walk H_x rows (flat_eval_pays() of the tables, or the autotuner's choice)
+  int variant;                // compiled register-budget variant (0 or 1)
+  int variant_f32, flat_eval_f32;  // the FP32 phase's choices in mixed precision
   const uint64_t* hx_terms;   // device
   const uint16_t* hx_off;     // device [N*N+1]
   const uint64_t* ht_terms;   // device

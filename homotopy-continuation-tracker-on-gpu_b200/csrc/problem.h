@@ -50,9 +50,25 @@ struct Problem {
   bool has_terms = false;
   std::vector<P2CTerm> p2c;
   std::vector<int> p2c_k_off;  // [M+1]
+  // launch tuning per precision (0: FP64, 1: FP32), set by ghc_autotune / ghc_set_tuning:
+  // compiled register-budget variant and H_x walk (-1: flat_eval_pays() decides)
+  int tune_variant[2] = {0, 0};
+  int tune_flat[2] = {-1, -1};
   DeviceTables dev;
   ~Problem();
 };
+
+// the problem's tuning into a launch of `precision` (the FP32 phase's choices for mixed)
+inline void apply_tuning(const Problem& pb, int precision, TrackParams& p) {
+  const int heur = flat_eval_pays(pb.hx_off.data(), pb.N);
+  const int f64 = pb.tune_flat[0] >= 0 ? pb.tune_flat[0] : heur;
+  const int f32 = pb.tune_flat[1] >= 0 ? pb.tune_flat[1] : heur;
+  const bool fp32 = precision == PREC_FP32;
+  p.variant = fp32 ? pb.tune_variant[1] : pb.tune_variant[0];
+  p.flat_eval = fp32 ? f32 : f64;
+  p.variant_f32 = pb.tune_variant[1];
+  p.flat_eval_f32 = f32;
+}
 
 // All return GHC_OK or a negative error code and set the thread's error message.
 int load_problem(const std::string& root, const std::string& name, Problem& pb);

@@ -48,6 +48,8 @@ int launch_track(const TrackParams& p, int precision, double t_switch, void* str
       TrackParams a = p;
       a.t_handover = std::min(t_switch, kMixedMaxSwitch);
       a.fail_limit = kMixedFailLimit;
+      a.variant = p.variant_f32;
+      a.flat_eval = p.flat_eval_f32;
       a.corr_tol2 = std::max(p.corr_tol2, kMixedF32Tol2);
       a.start_other = 1;        // double start solutions into the FP32 tracker
       a.ld_out = 2 * p.ld_out;  // float track in the first half of each double slot

@@ -508,12 +508,19 @@ __device__ __forceinline__ cx<R> load_cx(const void* base, bool f64, long long i
 }
 
 // CTAs per SM the tracker asks the register allocator for: the row of H_x (N
-// complex values) dominates the registers, so small systems afford more.
-// Measured on B200: FP64 N = 3 best at 6 (64 registers spill), N = 6 and N = 12 at 4.
-template <int N, typename R>
+// complex values) dominates the registers, so small systems afford more.  Two
+// compiled variants per size and precision; the autotuner (ghc_autotune) picks
+// one per problem.  Variant 0 is the best of B200 sweeps over the shipped
+// problems (FP64 N = 3 at 6 -- at 8 the 64 registers spill --, N = 6 and
+// N = 12 at 4); variant 1 trades registers for one more CTA per SM (N = 12:
+// better for the uncalibrated trifocal problem, worse for the generalized
+// 3-view problem, which have the same size).
+template <int N, typename R, int V>
 constexpr int track_min_blocks() {
-  return sizeof(R) == 8 ? (N <= 4 ? 6 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
-                        : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 3);
+  return V == 0 ? (sizeof(R) == 8 ? (N <= 4 ? 6 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
+                                  : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 3))
+                : (sizeof(R) == 8 ? (N <= 4 ? 8 : N <= 12 ? 5 : N <= 18 ? 4 : 3)
+                                  : (N <= 8 ? 6 : N <= 12 ? 5 : N <= 18 ? 3 : 2));
 }
 
 __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64_t* g_hx, const uint16_t* g_hxo,
@@ -553,12 +560,12 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 // with step dt_in[i] and the step / corrector counts already in steps / corr.
 // -------------------------------------------------------------------------------------------------
 #ifdef GHC_TRACK_MIN_BLOCKS
-#define GHC_MINB(N, R) GHC_TRACK_MIN_BLOCKS
+#define GHC_MINB(N, R, V) GHC_TRACK_MIN_BLOCKS
 #else
-#define GHC_MINB(N, R) track_min_blocks<N, R>()
+#define GHC_MINB(N, R, V) track_min_blocks<N, R, V>()
 #endif
-template <typename R, int N, int W, int KIND>
-__global__ void __launch_bounds__(128, GHC_MINB(N, R)) track_kernel(const TrackParams p) {
+template <typename R, int N, int W, int KIND, int V>
+__global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const TrackParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Tables tb = stage_tables(smem, p.hx_terms, p.hx_off, p.ht_terms, p.ht_off, N, p.n_hx_terms, p.n_ht_terms);
 

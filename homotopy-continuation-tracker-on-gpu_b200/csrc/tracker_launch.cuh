@@ -10,10 +10,10 @@ namespace launch_detail {
 
 constexpr int kBlock = 128;
 
-template <typename R, int N, int KIND>
+template <typename R, int N, int KIND, int V>
 int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
   constexpr int W = (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
-  auto kern = dev::track_kernel<R, N, W, KIND>;
+  auto kern = dev::track_kernel<R, N, W, KIND, V>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
   const bool flat = dev::kFlatAlways<N> || p.flat_eval;
@@ -58,25 +58,35 @@ int launch_polish_t(const PolishParams& p, cudaStream_t s) {
 #define GHC_P2C_SIZES(X) X(3) X(4) X(5) X(6) X(8) X(10) X(11) X(12) X(16) X(18)
 
 // dispatch of one precision mode over the compiled sizes
-template <typename R>
+template <typename R, int V>
 int launch_mode(const TrackParams& p, cudaStream_t s, int n_sm) {
   using namespace launch_detail;
   if (p.kind == KIND_P2C) {
     switch (p.N) {
 #define CASE(n) \
   case n:       \
-    return launch_track_t<R, n, KIND_P2C>(p, s, n_sm);
+    return launch_track_t<R, n, KIND_P2C, V>(p, s, n_sm);
       GHC_P2C_SIZES(CASE)
 #undef CASE
       default:
         return -10;
     }
   }
-  if (p.kind == KIND_PH && p.N == 30) return launch_track_t<R, 30, KIND_PH>(p, s, n_sm);
+  if (p.kind == KIND_PH && p.N == 30) return launch_track_t<R, 30, KIND_PH, V>(p, s, n_sm);
   return -10;
 }
 
-int launch_track_fp64(const TrackParams& p, cudaStream_t s, int n_sm);
-int launch_track_fp32(const TrackParams& p, cudaStream_t s, int n_sm);
+// one translation unit per (precision, variant): tracker_fp64.cu, tracker_fp64_v1.cu, tracker_fp32.cu,
+// tracker_fp32_v1.cu; launch_track_fp64 / _fp32 (tracker.cu) pick by TrackParams::variant
+int launch_track_fp64_v0(const TrackParams& p, cudaStream_t s, int n_sm);
+int launch_track_fp64_v1(const TrackParams& p, cudaStream_t s, int n_sm);
+int launch_track_fp32_v0(const TrackParams& p, cudaStream_t s, int n_sm);
+int launch_track_fp32_v1(const TrackParams& p, cudaStream_t s, int n_sm);
+inline int launch_track_fp64(const TrackParams& p, cudaStream_t s, int n_sm) {
+  return p.variant ? launch_track_fp64_v1(p, s, n_sm) : launch_track_fp64_v0(p, s, n_sm);
+}
+inline int launch_track_fp32(const TrackParams& p, cudaStream_t s, int n_sm) {
+  return p.variant ? launch_track_fp32_v1(p, s, n_sm) : launch_track_fp32_v0(p, s, n_sm);
+}
 
 }  // namespace ghc

@@ -43,6 +43,10 @@ class Counts(ctypes.Structure):
     _fields_ = [("converged", _I32), ("real", _I32), ("infinity", _I32), ("unique", _I32)]
 
 
+class TuneChoice(ctypes.Structure):
+    _fields_ = [("variant", _I32), ("flat", _I32), ("ms", ctypes.c_double), ("candidates", _I32)]
+
+
 class TrackArgs(ctypes.Structure):
     _fields_ = [("n_hyp", _I64), ("precision", _I32), ("max_steps", _I32), ("max_corr", _I32),
                 ("incr_steps", _I32), ("t_switch", ctypes.c_double), ("polish_iters", _I32),
@@ -72,6 +76,9 @@ ghc_p2c = _sig("ghc_p2c", ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int])
 ghc_p2c_device = _sig("ghc_p2c_device", ctypes.c_int, [_P, _I64, _P, _P, _P, _P, ctypes.c_int, _P])
 ghc_track = _sig("ghc_track", ctypes.c_int, [_P, ctypes.POINTER(TrackArgs), _P])
 ghc_track_noalloc = _sig("ghc_track_noalloc", ctypes.c_int, [_P, ctypes.POINTER(TrackArgs), _P])
+ghc_autotune = _sig("ghc_autotune", ctypes.c_int, [_P, ctypes.POINTER(TrackArgs), _P, ctypes.POINTER(TuneChoice)])
+ghc_set_tuning = _sig("ghc_set_tuning", ctypes.c_int, [_P, _I32, _I32, _I32])
+ghc_get_tuning = _sig("ghc_get_tuning", ctypes.c_int, [_P, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)])
 ghc_count_results = _sig("ghc_count_results", ctypes.c_int,
                          [_I32, _I32, _P, _P, _P, ctypes.c_double, ctypes.c_double, ctypes.POINTER(Counts)])
 ghc_count_results_device = _sig("ghc_count_results_device", ctypes.c_int,
@@ -206,6 +213,38 @@ def track(pb, ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, 
     step: optional dict(corr_tol2=, first_tol2=, dt_max=) step control; the
     default is the reference's (see ROBUST_STEP for the path-jump-free one).
     """
+    a = _track_args(ws, d_start_sols, d_coef_hx, d_coef_ht, d_p_start, d_p_target, d_p_diff, t_switch,
+                    polish_iters, max_steps, max_corr, incr_steps, want_resid, step)
+    if no_alloc:
+        # ghc_track_noalloc: counter and tables in the library's fixed device array
+        a.d_counter = None
+        _check(ghc_track_noalloc(pb.h, ctypes.byref(a), _stream()), "ghc_track_noalloc")
+    else:
+        _check(ghc_track(pb.h, ctypes.byref(a), _stream()), "ghc_track")
+
+
+def autotune(pb, ws, d_start_sols, **kw):
+    """Time the launch choices on this sample batch (track's arguments; outputs overwritten),
+    keep the fastest in the problem handle for the workspace's precision and return it
+    as dict(variant, flat, ms, candidates).  Synchronises torch's current stream."""
+    a = _track_args(ws, d_start_sols, **kw)
+    out = TuneChoice()
+    _check(ghc_autotune(pb.h, ctypes.byref(a), _stream(), ctypes.byref(out)), "ghc_autotune")
+    return dict(variant=out.variant, flat=out.flat, ms=out.ms, candidates=out.candidates)
+
+
+def set_tuning(pb, precision, variant, flat=-1):
+    _check(ghc_set_tuning(pb.h, precision, variant, flat), "ghc_set_tuning")
+
+
+def get_tuning(pb, precision):
+    v, f = _I32(), _I32()
+    _check(ghc_get_tuning(pb.h, precision, ctypes.byref(v), ctypes.byref(f)), "ghc_get_tuning")
+    return v.value, f.value
+
+
+def _track_args(ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, d_p_target=None, d_p_diff=None,
+                t_switch=0.9, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False, step=None):
     a = TrackArgs()
     a.n_hyp = ws.n_hyp
     a.precision = ws.precision
@@ -226,12 +265,7 @@ def track(pb, ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, 
     a.d_resid = ws.resid.data_ptr() if (want_resid or polish_iters > 0) and ws.precision != PREC_FP32 else None
     a.d_counter = ws.counter.data_ptr()
     a.paths = ws.paths
-    if no_alloc:
-        # ghc_track_noalloc: counter and tables in the library's fixed device array
-        a.d_counter = None
-        _check(ghc_track_noalloc(pb.h, ctypes.byref(a), _stream()), "ghc_track_noalloc")
-    else:
-        _check(ghc_track(pb.h, ctypes.byref(a), _stream()), "ghc_track")
+    return a
 
 
 def measure_fma_peak(precision=PREC_FP64):
@@ -253,18 +287,21 @@ def count_results(endpoints, conv, inf, imag_tol=1e-4, dup_tol=1e-4):
     return dict(converged=out.converged, real=out.real, infinity=out.infinity, unique=out.unique)
 
 
-def count_results_device(ws, N, imag_tol=1e-4, dup_tol=1e-4, want_class=False):
+def count_results_device(ws, N, imag_tol=1e-4, dup_tol=1e-4, want_class=False, out=None, class_out=None):
     """Counts of every hypothesis of a workspace, on the device (torch's current stream).
 
     Returns (counts int32 tensor [n_hyp, 4] = converged, real, infinity, unique;
     class uint8 tensor [n_hyp * paths] or None): bit 0 converged, bit 1 real,
     bit 2 counted as unique.  Needs FP64 endpoints (FP64 or mixed workspace).
+    out / class_out: preallocated int32 [>= n_hyp, 4] / uint8 [>= n_hyp * paths] device tensors.
     """
     import torch
     if ws.endpoints.dtype != torch.float64:
         raise GhcError("count_results_device needs FP64 endpoints")
-    counts = torch.zeros((ws.n_hyp, 4), dtype=torch.int32, device=ws.endpoints.device)
-    cls = torch.zeros(ws.n_hyp * ws.paths, dtype=torch.uint8, device=ws.endpoints.device) if want_class else None
+    counts = out if out is not None else torch.zeros((ws.n_hyp, 4), dtype=torch.int32, device=ws.endpoints.device)
+    cls = class_out
+    if cls is None and want_class:
+        cls = torch.zeros(ws.n_hyp * ws.paths, dtype=torch.uint8, device=ws.endpoints.device)
     _check(ghc_count_results_device(N, ws.paths, ws.n_hyp, ws.endpoints.data_ptr(), ws.conv.data_ptr(),
                                     ws.inf.data_ptr(), imag_tol, dup_tol, counts.data_ptr(),
                                     None if cls is None else cls.data_ptr(), _stream()), "ghc_count_results_device")

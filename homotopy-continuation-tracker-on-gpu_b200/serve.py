@@ -13,12 +13,16 @@ from pinned host memory, builds the coefficient tables on the device and
 launches the tracker on the problem's stream -- while batches of the other
 problems (and the other slot of the same problem) are still running.  When a
 batch's event has completed, each request's slice of the endpoints and flags
-is copied back and the request is complete.  Results do not depend on which
-other requests shared a launch: every hypothesis is tracked with the same
-arithmetic alone or in a batch (tests/test_gpu_serve.py checks this).
+is copied back and the request is complete, with its per-hypothesis result
+counts (converged, real, infinity, unique) computed on the device.  Results do
+not depend on which other requests shared a launch: every hypothesis is tracked
+with the same arithmetic alone or in a batch (tests/test_gpu_serve.py checks this).
 
+``precision`` selects the tracker (plain FP64 or the two-phase mixed one);
+``tune=True`` autotunes each problem's launch on a sample batch at start-up.
 ``sequential=True`` gives the baseline of the same GPU without batching: one
-request per launch, one stream, FIFO.
+request per launch, one stream, FIFO; ``dropin_rate`` measures the drop-in's
+one hypothesis per launch.
 """
 import collections
 import json
@@ -33,30 +37,35 @@ MIX = ["P3P_TD", "5pt_rel_pos_alg_form_quat", "generalized_3views_4pts", "trifoc
 
 
 class Request:
-    __slots__ = ("rid", "problem", "targets", "arrival", "done", "endpoints", "conv", "status")
+    __slots__ = ("rid", "problem", "targets", "arrival", "done", "endpoints", "conv", "inf", "status", "counts")
 
     def __init__(self, rid, problem, targets, arrival):
         self.rid, self.problem, self.targets, self.arrival = rid, problem, targets, arrival
         self.done = None
-        self.endpoints = self.conv = self.status = None
+        # endpoints [n * paths, N], conv / inf / status [n * paths]; counts [n, 4] per hypothesis
+        # (converged, real, infinity, unique; computed on the device)
+        self.endpoints = self.conv = self.inf = self.status = self.counts = None
 
 
 class _Slot:
-    def __init__(self, torch, pb, cap, paths, N, P1):
+    def __init__(self, torch, pb, cap, paths, N, P1, precision):
         self.cap = cap
         self.h_tg = torch.zeros((cap, P1, 2), dtype=torch.float64).pin_memory()
         self.d_tg = torch.zeros((cap, P1, 2), dtype=torch.float64, device="cuda")
         self.d_diff = torch.zeros((cap, P1, 2), dtype=torch.float64, device="cuda")
-        self.ws = ghc.Workspace(pb, cap, ghc.PREC_FP64, paths=paths)
+        self.ws = ghc.Workspace(pb, cap, precision, paths=paths)
+        self.d_counts = torch.zeros((cap, 4), dtype=torch.int32, device="cuda")
+        self.h_counts = torch.zeros((cap, 4), dtype=torch.int32).pin_memory()
         self.h_ep = torch.zeros((cap * paths, N, 2), dtype=torch.float64).pin_memory()
         self.h_conv = torch.zeros(cap * paths, dtype=torch.uint8).pin_memory()
+        self.h_inf = torch.zeros(cap * paths, dtype=torch.uint8).pin_memory()
         self.h_status = torch.zeros(cap * paths, dtype=torch.uint8).pin_memory()
         self.event = None
         self.requests = []
 
 
 class _Problem:
-    def __init__(self, torch, name, cap, slots):
+    def __init__(self, torch, name, cap, slots, precision):
         self.name = name
         self.pb = ghc.Problem(name)
         s, t = self.pb.params()
@@ -69,19 +78,43 @@ class _Problem:
         sols = self.pb.start_sols()
         self.d_sols = torch.from_numpy(np.stack([sols.real, sols.imag], -1).copy()).cuda()
         self.stream = torch.cuda.Stream()
-        self.slots = [_Slot(torch, self.pb, cap, self.paths, self.pb.N, self.pb.P + 1) for _ in range(slots)]
+        self.slots = [_Slot(torch, self.pb, cap, self.paths, self.pb.N, self.pb.P + 1, precision)
+                      for _ in range(slots)]
         self.queue = collections.deque()
+        self.tuning = None
+
+    def sample_targets(self, n, seed):
+        if self.name == "P3P_TD":
+            return scenes.p3p_td(n, seed=seed)[0][1]
+        return scenes.perturbed_targets(self.target, n, seed=seed)
+
+    def inputs(self, torch, slot, n):
+        if self.pb.kind == ghc.KIND_P2C:
+            hx, ht = self.pb.p2c_device(self.d_start, slot.d_tg[:n])
+            return dict(d_coef_hx=hx, d_coef_ht=ht)
+        torch.sub(slot.d_tg[:n], self.d_start[None], out=slot.d_diff[:n])
+        return dict(d_p_start=self.d_start, d_p_target=slot.d_tg[:n], d_p_diff=slot.d_diff[:n])
+
+    def tune(self, torch, n=128):
+        """Autotune this problem's launch on a sample batch of n hypotheses (at start-up)."""
+        slot = self.slots[0]
+        n = min(n, slot.cap)
+        tg = self.sample_targets(n, seed=4711)
+        slot.d_tg[:n].copy_(torch.from_numpy(np.stack([tg.real, tg.imag], -1)))
+        slot.ws.n_hyp = n
+        self.tuning = ghc.autotune(self.pb, slot.ws, self.d_sols, **self.inputs(torch, slot, n))
 
 
 def bytes_per_hypothesis(pb):
     P1 = pb.P + 1
     tables = 16 * (pb.M + 1) * (2 * pb.K + 1) if pb.kind == ghc.KIND_P2C else 0
     per_path = 16 * pb.N + 3 + 4 * 2 + 8 * 3
-    return 2 * 16 * P1 + tables + pb.paths * (per_path + 16 * pb.N + 2)
+    return 2 * 16 * P1 + tables + 2 * 16 + pb.paths * (per_path + 16 * pb.N + 3)
 
 
 class Server:
-    def __init__(self, torch, problems=MIX, max_batch=2048, hbm_fraction=0.25, sequential=False, max_request=512):
+    def __init__(self, torch, problems=MIX, max_batch=2048, hbm_fraction=0.25, sequential=False, max_request=512,
+                 tune=False, precision=ghc.PREC_FP64):
         self.torch = torch
         self.sequential = sequential
         free, _ = torch.cuda.mem_get_info()
@@ -94,9 +127,12 @@ class Server:
             if cap < max_request:
                 raise MemoryError("%s: %d hypotheses per slot fit in the memory budget, requests may have %d"
                                   % (name, cap, max_request))
-            self.problems[name] = _Problem(torch, name, cap, slots)
+            self.problems[name] = _Problem(torch, name, cap, slots, precision)
         self.fifo = collections.deque()  # sequential mode: global order
         self.launches = 0
+        if tune:
+            for prob in self.problems.values():
+                prob.tune(torch)
 
     def submit(self, req):
         cap = self.problems[req.problem].slots[0].cap
@@ -118,16 +154,13 @@ class Server:
             slot.d_tg[:n].copy_(slot.h_tg[:n], non_blocking=True)
             ws = slot.ws
             ws.n_hyp = n
-            if prob.pb.kind == ghc.KIND_P2C:
-                hx, ht = prob.pb.p2c_device(prob.d_start, slot.d_tg[:n])
-                ghc.track(prob.pb, ws, prob.d_sols, d_coef_hx=hx, d_coef_ht=ht)
-            else:
-                torch.sub(slot.d_tg[:n], prob.d_start[None], out=slot.d_diff[:n])
-                ghc.track(prob.pb, ws, prob.d_sols, d_p_start=prob.d_start, d_p_target=slot.d_tg[:n],
-                          d_p_diff=slot.d_diff[:n])
+            ghc.track(prob.pb, ws, prob.d_sols, **prob.inputs(torch, slot, n))
+            ghc.count_results_device(ws, prob.pb.N, out=slot.d_counts[:n])
+            slot.h_counts[:n].copy_(slot.d_counts[:n], non_blocking=True)
             m = n * prob.paths
             slot.h_ep[:m].copy_(ws.endpoints[:m], non_blocking=True)
             slot.h_conv[:m].copy_(ws.conv[:m], non_blocking=True)
+            slot.h_inf[:m].copy_(ws.inf[:m], non_blocking=True)
             slot.h_status[:m].copy_(ws.status[:m], non_blocking=True)
             slot.event = torch.cuda.Event()
             slot.event.record(prob.stream)
@@ -135,11 +168,16 @@ class Server:
 
     def _complete(self, prob, slot, now):
         off = 0
+        hoff = 0
         for r in slot.requests:
-            m = r.targets.shape[0] * prob.paths
+            nh = r.targets.shape[0]
+            r.counts = slot.h_counts[hoff:hoff + nh].numpy().copy()
+            hoff += nh
+            m = nh * prob.paths
             e = slot.h_ep[off:off + m].numpy()
             r.endpoints = e[..., 0] + 1j * e[..., 1]
             r.conv = slot.h_conv[off:off + m].numpy().copy()
+            r.inf = slot.h_inf[off:off + m].numpy().copy()
             r.status = slot.h_status[off:off + m].numpy().copy()
             r.done = now
             off += m
@@ -194,9 +232,7 @@ def run_stream(server, lam, n_req, seed=0):
     reqs = []
     for i in range(n_req):
         prob = server.problems[probs[i]]
-        tg = scenes.perturbed_targets(prob.target, int(sizes[i]), seed=seed * 100003 + i) \
-            if probs[i] != "P3P_TD" else scenes.p3p_td(int(sizes[i]), seed=seed * 100003 + i)[0][1]
-        reqs.append(Request(i, probs[i], tg, None))
+        reqs.append(Request(i, probs[i], prob.sample_targets(int(sizes[i]), seed=seed * 100003 + i), None))
     server.torch.cuda.synchronize()
     t0 = time.perf_counter()
     nxt = 0
@@ -216,32 +252,57 @@ def run_stream(server, lam, n_req, seed=0):
     return lat, int(sizes.sum()), wall, reqs
 
 
+def dropin_rate(server, n, seed=0):
+    """One hypothesis per launch, FIFO on one stream: the drop-in tracker's service rate
+    on the stream's problem mix (hypotheses/s over n single-hypothesis requests)."""
+    rng = np.random.default_rng(seed)
+    names = list(server.problems)
+    reqs = [Request(i, names[k], server.problems[names[k]].sample_targets(1, seed=seed * 7919 + i), 0.0)
+            for i, k in enumerate(rng.integers(0, len(names), size=n))]
+    server.torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in reqs:
+        server.submit(r)
+    while server.step(time.perf_counter() - t0):
+        pass
+    return n / (time.perf_counter() - t0)
+
+
+def _stats(lat, hyp, wall):
+    return {"throughput": hyp / wall, "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+            "p99_ms": 1e3 * float(np.percentile(lat, 99)), "wall_s": wall}
+
+
 def bench(args, torch):
     torch.cuda.set_device(0)
     lams = [100, 300, 1000, 3000, 10000, 20000]
     n_req = 60
+    tune = bool(getattr(args, "tune", 1))
+    modes = {"batched_fp64": Server(torch, tune=tune),
+             "batched_mixed": Server(torch, tune=tune, precision=ghc.PREC_MIXED),
+             "sequential_fp64": Server(torch, sequential=True, tune=tune)}
+    for i, srv in enumerate(modes.values()):  # warm-up (kernel attributes, tables)
+        run_stream(srv, 1000, 8, seed=990 + i)
     rows = []
-    batched = Server(torch)
-    seq = Server(torch, sequential=True)
-    # warm both (kernel attributes, tables) with a small stream
-    run_stream(batched, 1000, 8, seed=999)
-    run_stream(seq, 1000, 4, seed=998)
     for lam in lams:
-        lat, hyp, wall, _ = run_stream(batched, lam, n_req, seed=lam)
-        lat_s, hyp_s, wall_s, _ = run_stream(seq, lam, n_req, seed=lam)
-        rows.append({"lambda_req_s": lam, "requests": n_req, "hypotheses": hyp,
-                     "batched": {"throughput": hyp / wall, "p50_ms": 1e3 * float(np.percentile(lat, 50)),
-                                 "p99_ms": 1e3 * float(np.percentile(lat, 99)), "wall_s": wall},
-                     "sequential_fp64": {"throughput": hyp_s / wall_s,
-                                         "p50_ms": 1e3 * float(np.percentile(lat_s, 50)),
-                                         "p99_ms": 1e3 * float(np.percentile(lat_s, 99)), "wall_s": wall_s}})
-    best = max(r["batched"]["throughput"] for r in rows)
+        row = {"lambda_req_s": lam, "requests": n_req}
+        for name, srv in modes.items():
+            lat, hyp, wall, _ = run_stream(srv, lam, n_req, seed=lam)
+            row["hypotheses"] = hyp
+            row[name] = _stats(lat, hyp, wall)
+        rows.append(row)
+    dropin = dropin_rate(modes["sequential_fp64"], 64, seed=5)
+    best = max(max(r["batched_fp64"]["throughput"], r["batched_mixed"]["throughput"]) for r in rows)
     line = {"metric": "served hypothesis-solves/s and p50/p99 request latency vs offered load", "value": best,
             "unit": "hypotheses/s", "n_gpus": 1, "steps": len(lams), "warmup": 1, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic (seeded)",
             "config": {"workload": "Poisson request stream, %d requests per load point, 1-512 hypotheses "
                                    "(log-uniform) of a problem drawn uniformly from %s; continuous batching "
-                                   "on per-problem streams vs one-request-per-launch FP64" % (n_req, MIX)},
-            "capacity_hypotheses_per_launch": {n: p.slots[0].cap for n, p in batched.problems.items()},
+                                   "on per-problem streams (FP64 and mixed) vs one request per launch (FP64) vs "
+                                   "one hypothesis per launch (the drop-in, FP64)" % (n_req, MIX)},
+            "capacity_hypotheses_per_launch": {n: p.slots[0].cap for n, p in modes["batched_fp64"].problems.items()},
+            "dropin_one_hypothesis_per_launch": {"throughput": dropin, "hypotheses": 64},
+            "best_vs_dropin": best / dropin,
+            "tuning": {n: p.tuning for n, p in modes["batched_fp64"].problems.items()},
             "sweep": rows}
     print(json.dumps(line), flush=True)

@@ -71,13 +71,19 @@ class Batch:
         if step:
             self.kw.update(step)
 
-    def launch(self):
+    def _inputs(self):
         if self.pb.kind == ghc.KIND_P2C:
             hx, ht = self.pb.p2c_device(self.d_start, self.d_tg)
-            ghc.track(self.pb, self.ws, self.d_sols, d_coef_hx=hx, d_coef_ht=ht, **self.kw)
-        else:
-            ghc.track(self.pb, self.ws, self.d_sols, d_p_start=self.d_start, d_p_target=self.d_tg,
-                      d_p_diff=self.d_diff, **self.kw)
+            return dict(d_coef_hx=hx, d_coef_ht=ht)
+        return dict(d_p_start=self.d_start, d_p_target=self.d_tg, d_p_diff=self.d_diff)
+
+    def launch(self):
+        ghc.track(self.pb, self.ws, self.d_sols, **self._inputs(), **self.kw)
+
+    def tune(self):
+        """Autotune the launch on this batch (before any capture); returns the choice."""
+        self.tuning = ghc.autotune(self.pb, self.ws, self.d_sols, **self._inputs(), **self.kw)
+        return self.tuning
 
 
 def _time_graph(torch, g, steps, flush):
@@ -113,6 +119,7 @@ def config_cy(args, torch):
     b = Batch(torch, "uncalibrated_trifocal_rel_pos_CY", H, 1000 + args.seed, polish=2, scene={"noise_px": 0.0})
     _, _, inlier = scenes.uncalibrated_trifocal_rel_pos_CY(H, seed=1000 + args.seed, noise_px=0.0)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    tuning = b.tune() if args.tune else None
     g = _capture(torch, b.launch)
     for _ in range(args.warmup):
         g.replay()
@@ -142,7 +149,7 @@ def config_cy(args, torch):
           paths={"per_step": H * b.paths, "converged_frac": float(conv.mean()), "mean_steps": float(steps.mean()),
                  "max_steps": int(steps.max())},
           inlier_hypotheses=int(inlier.sum()), inlier_ground_truth_found=found / max(1, int(inlier.sum())),
-          gpu_launches=3 * args.steps)
+          tuning=tuning, gpu_launches=3 * args.steps)
 
 
 def config_p3p_td(args, torch):
@@ -161,6 +168,7 @@ def config_p3p_td(args, torch):
     gt_ok = bool(np.abs(E - single.truth[0]).max(axis=1).min() < 1e-9)
     H = 65536
     batch = Batch(torch, "P3P_TD", H, 8 + args.seed, polish=2)
+    tuning = batch.tune() if args.tune else None
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     g = _capture(torch, batch.launch)
     for _ in range(args.warmup):
@@ -174,7 +182,7 @@ def config_p3p_td(args, torch):
           ms_per_step=sum(ms) / len(ms), single_instance={"p50_ms": float(np.percentile(lat, 50)),
                                                           "p99_ms": float(np.percentile(lat, 99)),
                                                           "ground_truth_found": gt_ok},
-          ground_truth_found_frac=float(hit), gpu_launches=3 * args.steps)
+          ground_truth_found_frac=float(hit), tuning=tuning, gpu_launches=3 * args.steps)
 
 
 MIX = [("P3P_TD", 8192), ("5pt_rel_pos_alg_form_quat", 4096), ("generalized_3views_4pts", 2048),
@@ -183,6 +191,7 @@ MIX = [("P3P_TD", 8192), ("5pt_rel_pos_alg_form_quat", 4096), ("generalized_3vie
 
 def config_mix(args, torch):
     batches = [Batch(torch, n, h, 50 + i + args.seed) for i, (n, h) in enumerate(MIX)]
+    tuning = {b.name: b.tune() for b in batches} if args.tune else None
     streams = [torch.cuda.Stream() for _ in batches]
 
     def fork_join():
@@ -211,6 +220,7 @@ def config_mix(args, torch):
           {"workload": "uneven mix in one CUDA graph: " + ", ".join("%s %d hyp" % m for m in MIX) +
                        "; four streams forked and joined inside the graph; FP64, reference step control"},
           ms_per_step=sum(ms) / len(ms), alone_ms=alone, sum_alone_ms=sum(alone.values()),
+          tuning=tuning,
           per_problem={b.name: {"hypotheses": b.H, "paths": b.H * b.paths,
                                 "converged_frac": float(b.ws.conv.float().mean())} for b in batches},
           gpu_launches=8 * args.steps)
@@ -230,6 +240,8 @@ def config_g3v4_mono(args, torch):
     for name, prec in (("fp64", ghc.PREC_FP64), ("mixed", ghc.PREC_MIXED)):
         b = Batch(torch, "generalized_3views_4pts", H, 77 + args.seed, precision=prec, polish=3, step=step,
                   start=q, sols=Sq)
+        if args.tune:
+            b.tune()
         g = _capture(torch, b.launch)
         ms = _time_graph(torch, g, max(1, args.steps // 2), flush)
         runs[name] = (_to_cx(b.ws.endpoints).reshape(H, b.paths, -1), b.ws.conv.cpu().numpy().reshape(H, -1) == 1,
@@ -264,6 +276,7 @@ def config_problem(args, torch):
         step = dict(step=dict(corr_tol2=1e-12, first_tol2=1e-2, dt_max=0.05), max_corr=3, max_steps=2000)
     H = args.hyp
     b = Batch(torch, args.problem, H, 500 + args.seed, precision=prec, step=step)
+    tuning = b.tune() if args.tune else None
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     g = _capture(torch, b.launch)
     for _ in range(args.warmup):
@@ -279,6 +292,7 @@ def config_problem(args, torch):
           paths={"per_step": H * b.paths, "converged_frac": float(b.ws.conv.float().mean()),
                  "mean_solves": float(solves.mean()), "p99_solves": float(np.percentile(solves, 99)),
                  "max_solves": int(solves.max())},
+          tuning=tuning,
           solves_per_s=float(solves.sum()) / (statistics.median(ms) * 1e-3), gpu_launches=len(ms) * (2 if
           b.pb.kind == ghc.KIND_P2C else 1))
 

@@ -159,6 +159,35 @@ int ghc_track(const ghc_problem* pb, const ghc_track_args* args, void* stream);
 int ghc_track_noalloc(const ghc_problem* pb, const ghc_track_args* args, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Launch tuning.  The reference fixes threads-per-path and block shape per
+ * problem in its 21 hand-written wrappers (e.g. kernel_HC_Solver_P3P.cu:284-297:
+ * one block of N threads per path); here the sub-warp width follows N and two
+ * things are chosen per problem handle and precision:
+ *   variant  the compiled register budget (0: the default table of CTAs per SM,
+ *            1: one more CTA per SM with fewer registers per thread);
+ *   flat     how H_x is walked (1: each lane walks its row once through a
+ *            shared-memory scratch row, 0: one loop per column; -1: chosen from
+ *            the table structure; above 16 unknowns always 1).
+ * Every choice computes bit-identical results; only the speed differs.
+ *
+ * ghc_autotune runs the caller's sample batch (`sample`, exactly as for
+ * ghc_track, outputs overwritten) once per candidate after a warm-up, times it
+ * with CUDA events on `stream`, keeps the fastest in the handle for
+ * sample->precision (mixed: both phases) and returns it.  It synchronises
+ * `stream`; do not run it while the handle is tracking elsewhere.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t variant, flat;
+  double ms;                  /* the sample's time with this choice */
+  int32_t candidates;         /* how many were timed */
+} ghc_tune_choice;
+
+int ghc_autotune(ghc_problem* pb, const ghc_track_args* sample, void* stream, ghc_tune_choice* best);
+/* precision GHC_PREC_FP64 or GHC_PREC_FP32 (GHC_PREC_MIXED: both) */
+int ghc_set_tuning(ghc_problem* pb, int32_t precision, int32_t variant, int32_t flat);
+int ghc_get_tuning(const ghc_problem* pb, int32_t precision, int32_t* variant, int32_t* flat);
+
+/* ---------------------------------------------------------------------------
  * Result counts of one hypothesis on the host.
  * Replaces Evaluations::Evaluate_GPUHC_Sols and Evaluations::Find_Unique_Sols
  * (GPU-HC/magmaHC/Evaluations.cpp:88-110, 127-176).  h_endpoints [paths][N].

@@ -38,6 +38,43 @@ def test_requests_same_alone_and_in_the_mix():
         assert np.array_equal(ws.conv.cpu().numpy(), r.conv)
         fin = np.isfinite(e)
         assert np.array_equal(e[fin], r.endpoints[fin])
+        # per-hypothesis counts from the device equal the host rule on the returned endpoints
+        P = prob.paths
+        for h in range(n):
+            c = ghc.count_results(r.endpoints[h * P:(h + 1) * P], r.conv[h * P:(h + 1) * P], r.inf[h * P:(h + 1) * P])
+            assert [c["converged"], c["real"], c["infinity"], c["unique"]] == r.counts[h].tolist()
+
+
+def test_mixed_server_and_tuning_keep_results():
+    """A mixed-precision server gives each request what a mixed run alone gives; an
+    autotuned server gives bit-identical results to an untuned one."""
+    names = ["P3P_TD", "trifocal_2op1p_30x30"]
+    mixed = serve.Server(torch, problems=names, max_batch=512, precision=ghc.PREC_MIXED, tune=True)
+    _, _, _, reqs = serve.run_stream(mixed, lam=3000, n_req=6, seed=12)
+    for r in reqs:
+        prob = mixed.problems[r.problem]
+        n = r.targets.shape[0]
+        ws = ghc.Workspace(prob.pb, n, ghc.PREC_MIXED)
+        if prob.pb.kind == ghc.KIND_P2C:
+            hx, ht = prob.pb.p2c_device(prob.d_start, cx_t(r.targets))
+            ghc.track(prob.pb, ws, prob.d_sols, d_coef_hx=hx, d_coef_ht=ht)
+        else:
+            tg = cx_t(r.targets)
+            ghc.track(prob.pb, ws, prob.d_sols, d_p_start=prob.d_start, d_p_target=tg,
+                      d_p_diff=tg - prob.d_start[None])
+        torch.cuda.synchronize()
+        e = ws.endpoints.cpu().numpy()
+        e = e[..., 0] + 1j * e[..., 1]
+        fin = np.isfinite(e)
+        assert np.array_equal(ws.conv.cpu().numpy(), r.conv)
+        assert np.array_equal(e[fin], r.endpoints[fin])
+    tuned = serve.Server(torch, problems=["P3P_TD"], max_batch=512, tune=True)
+    plain = serve.Server(torch, problems=["P3P_TD"], max_batch=512)
+    assert tuned.problems["P3P_TD"].tuning["candidates"] == 4
+    _, _, _, rt = serve.run_stream(tuned, lam=5000, n_req=5, seed=9)
+    _, _, _, rp = serve.run_stream(plain, lam=5000, n_req=5, seed=9)
+    for x, y in zip(rt, rp):
+        assert np.array_equal(x.endpoints, y.endpoints) and np.array_equal(x.counts, y.counts)
 
 
 def test_sequential_baseline_matches_batched():

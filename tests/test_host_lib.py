@@ -149,3 +149,15 @@ def test_cli_help_and_missing_problem():
     assert r.returncode == 0 and "-p" in r.stdout
     r = subprocess.run([exe, "-p", "no_such_problem"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "DATA LOAD ERROR" in r.stderr
+
+
+def test_tuning_setters_validate():
+    pb = ghc.Problem("generalized_3views_4pts")
+    assert ghc.get_tuning(pb, ghc.PREC_FP64) == (0, -1)
+    ghc.set_tuning(pb, ghc.PREC_MIXED, 1, 0)
+    assert ghc.get_tuning(pb, ghc.PREC_FP64) == (1, 0) and ghc.get_tuning(pb, ghc.PREC_FP32) == (1, 0)
+    ghc.set_tuning(pb, ghc.PREC_FP32, 0, 1)
+    assert ghc.get_tuning(pb, ghc.PREC_FP64) == (1, 0) and ghc.get_tuning(pb, ghc.PREC_FP32) == (0, 1)
+    for bad in [(ghc.PREC_FP64, 2, 0), (ghc.PREC_FP64, 0, 2), (7, 0, 0)]:
+        with pytest.raises(ghc.GhcError):
+            ghc.set_tuning(pb, *bad)

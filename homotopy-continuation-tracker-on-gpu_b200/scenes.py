@@ -207,11 +207,89 @@ def seed_pair(name, seed=0):
     raise KeyError(name)
 
 
+def cayley(r):
+    """The unnormalised Cayley matrix M(r) of start-sys-gen/trifocal_2op1p_30x30_monodromySolve.jl:6-11;
+    M(r) / (1 + |r|^2) is a rotation."""
+    x, y, z = r
+    return np.array([[1 + x * x - (y * y + z * z), 2 * (x * y - z), 2 * (x * z + y)],
+                     [2 * (x * y + z), 1 + y * y - (x * x + z * z), 2 * (y * z - x)],
+                     [2 * (x * z - y), 2 * (y * z + x), 1 + z * z - (x * x + y * y)]])
+
+
+def trifocal_2op1p_30x30(n_hyp, seed=0, noise_px=0.0, image_px=1000.0, max_angle=0.4):
+    """Trifocal relative pose from three points, two of them with curve tangents (33 parameters,
+    30 unknowns) -- the system of auto-data-gen-tools/p2c-problems/sys_trifocal_2op1p_30x30.m as
+    built by start-sys-gen/trifocal_2op1p_30x30_monodromySolve.jl:13-80.
+
+    Scene: points X_1..X_3 in camera 1 at depth 4-8, unit 3D tangent directions D_1, D_2 at
+    X_1, X_2; cameras 2 and 3 with rotations R_v = M(r_v) / s_v (Cayley, s_v = 1 + |r_v|^2,
+    angle up to max_angle) and translations T_v ~ N(0, 0.5^2).
+    Parameters (the script's flatten order): image points x[p, v, :] for p = 1..3, v = 1..3
+    (c1..c18, normalised coordinates), image tangents d[p, v, :] for p = 1, 2 (c19..c30, unit 2D
+    directions), then a11 = depth of X_1 in camera 1, e11, e21 = z of D_1, D_2 (c31..c33).
+    Unknowns: a21, a31 (camera-1 depths of X_2, X_3), a12, a22, a32, a13, a23, a33 (camera-2/3
+    depths times s_v), e12, e13, e22, e23 (z of s_v R_v D_p), u11, u12, u13, u21, u22, u23
+    (tangent lengths: D_p in view v = e x_h + u [d; 0]), t2 = s_2 T_2, t3 = s_3 T_3, r2, r3.
+    Returns (targets [H, 34] with slot 33 = 1, truth [H, 30]); with noise_px = 0 the truth is an
+    exact solution (known-answer test).
+    """
+    rng = np.random.default_rng(seed)
+    sigma = noise_px / image_px
+    targets = np.zeros((n_hyp, 34), dtype=np.complex128)
+    truth = np.zeros((n_hyp, 30))
+    for h in range(n_hyp):
+        while True:
+            X = rng.uniform(-1, 1, size=(3, 3))
+            X[:, 2] += rng.uniform(4, 8, size=3)
+            D = rng.normal(size=(2, 3))
+            D /= np.linalg.norm(D, axis=1, keepdims=True)
+            r = {}
+            T = {}
+            R = {1: np.eye(3)}
+            for v in (2, 3):
+                k = rng.normal(size=3)
+                k /= np.linalg.norm(k)
+                r[v] = np.tan(rng.uniform(0, max_angle) / 2) * k  # Cayley parameter of that rotation
+                R[v] = cayley(r[v]) / (1 + r[v] @ r[v])
+                T[v] = 0.5 * rng.normal(size=3)
+            Y = {1: X}
+            for v in (2, 3):
+                Y[v] = X @ R[v].T + T[v]
+            if all(Y[v][:, 2].min() > 1.0 for v in (1, 2, 3)):
+                break
+        x = {v: Y[v][:, :2] / Y[v][:, 2:3] for v in (1, 2, 3)}
+        d, u, e = {}, {}, {}
+        for v in (1, 2, 3):
+            for p in (0, 1):
+                Dv = R[v] @ D[p]
+                g = Dv[:2] - Dv[2] * x[v][p]
+                d[p, v] = g / np.linalg.norm(g)
+                u[p, v] = np.linalg.norm(g)
+                e[p, v] = Dv[2]
+        xs = {v: x[v] + sigma * rng.normal(size=x[v].shape) for v in (1, 2, 3)}
+        c = []
+        for p in range(3):
+            for v in (1, 2, 3):
+                c += list(xs[v][p])
+        for p in (0, 1):
+            for v in (1, 2, 3):
+                c += list(d[p, v])
+        c += [Y[1][0, 2], e[0, 1], e[1, 1]]
+        targets[h, :33] = c
+        targets[h, 33] = 1.0
+        s = {v: 1 + r[v] @ r[v] for v in (2, 3)}
+        a = [Y[1][1, 2], Y[1][2, 2]] + [s[2] * Y[2][p, 2] for p in range(3)] + [s[3] * Y[3][p, 2] for p in range(3)]
+        ee = [s[2] * e[0, 2], s[3] * e[0, 3], s[2] * e[1, 2], s[3] * e[1, 3]]
+        uu = [u[0, 1], s[2] * u[0, 2], s[3] * u[0, 3], u[1, 1], s[2] * u[1, 2], s[3] * u[1, 3]]
+        truth[h] = np.concatenate([a, ee, uu, s[2] * T[2], s[3] * T[3], r[2], r[3]])
+    return targets, truth
+
+
 def perturbed_targets(target, n_hyp, seed=0, scale=0.05):
     """Seeded real perturbations of a problem's shipped target parameters (slot P kept at 1).
 
-    Stands in for scene generators not written here (5-point relative pose,
-    trifocal 30x30 from lines): real instances near the shipped one.
+    Stands in for the scene generator not written here (5-point relative pose):
+    real instances near the shipped one.
     """
     rng = np.random.default_rng(seed)
     base = np.asarray(target, dtype=np.complex128)[:-1].real
@@ -234,6 +312,9 @@ def targets_for(name, n_hyp, seed, start, shipped_target, **scene):
     if name == "P3P_TD":
         (st, tg), truth = p3p_td(n_hyp, seed=seed)
         return st, tg, truth
+    if name == "trifocal_2op1p_30x30":
+        tg, truth = trifocal_2op1p_30x30(n_hyp, seed=seed, **scene)
+        return start, tg, truth
     return start, perturbed_targets(shipped_target, n_hyp, seed=seed), None
 
 
@@ -241,4 +322,5 @@ GENERATORS = {
     "generalized_3views_4pts": generalized_3views_4pts,
     "uncalibrated_trifocal_rel_pos_CY": uncalibrated_trifocal_rel_pos_CY,
     "P3P_TD": p3p_td,
+    "trifocal_2op1p_30x30": trifocal_2op1p_30x30,
 }

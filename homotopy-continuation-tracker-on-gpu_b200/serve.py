@@ -86,6 +86,8 @@ class _Problem:
     def sample_targets(self, n, seed):
         if self.name == "P3P_TD":
             return scenes.p3p_td(n, seed=seed)[0][1]
+        if self.name in scenes.GENERATORS:
+            return scenes.GENERATORS[self.name](n, seed=seed)[0]
         return scenes.perturbed_targets(self.target, n, seed=seed)
 
     def inputs(self, torch, slot, n):

@@ -80,3 +80,25 @@ def test_generalized_3views_4pts_scene_known_answer():
                 max_corr=3, max_steps=2000)
     E = r["endpoints"][r["conv"] == 1]
     assert np.abs(E - gt[0]).max(axis=1).min() < 1e-9
+
+
+def test_trifocal_30x30_scene_known_answer():
+    """Scenes -> the 33 parameters of the Chicago-style trifocal system: the scene's unknowns
+    solve F(x; c) = 0, and tracking the shipped 312-path start system recovers them."""
+    pb = O.Problem("trifocal_2op1p_30x30")
+    tg, gt = scenes.trifocal_2op1p_30x30(3, seed=5)
+    for h in range(3):
+        H, _, _ = O.eval_system(pb, gt[h].astype(complex), 1.0, p_start=pb.start_params, p_target=tg[h])
+        assert np.abs(H).max() < 1e-12 * max(1.0, np.abs(gt[h]).max() ** 3)
+    r = O.track(pb, pb.start_sols, p_start=pb.start_params, p_target=tg[:1], polish_iters=3,
+                nthreads=os.cpu_count())
+    E = r["endpoints"][r["conv"] == 1]
+    assert np.abs(E - gt[0]).max(axis=1).min() < 1e-9 * np.abs(gt[0]).max()
+
+
+def test_cayley_is_a_scaled_rotation():
+    rng = np.random.default_rng(0)
+    for _ in range(5):
+        r = rng.normal(size=3)
+        R = scenes.cayley(r) / (1 + r @ r)
+        assert np.allclose(R @ R.T, np.eye(3), atol=1e-12) and abs(np.linalg.det(R) - 1) < 1e-12

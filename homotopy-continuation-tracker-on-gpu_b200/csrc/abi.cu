@@ -77,6 +77,7 @@ TrackParams base_params(const Problem& pb) {
   p.ht_terms = pb.dev.ht_terms;
   p.ht_off = pb.dev.ht_off;
   p.flat_eval = flat_eval_pays(pb.hx_off.data(), pb.N);
+  p.scr_slots = row_nonzeros_max(pb.hx_off.data(), pb.N);
   // the reference's step control (kernel_HC_Solver_P3P.cu:214): no contraction test, no step cap
   p.corr_tol2 = 1e-6;
   p.first_tol2 = HUGE_VAL;
@@ -95,6 +96,7 @@ PolishParams polish_params(const TrackParams& t, double* endpoints, const uint8_
   q.n_hx_terms = t.n_hx_terms;
   q.n_ht_terms = t.n_ht_terms;
   q.flat_eval = t.flat_eval;
+  q.scr_slots = t.scr_slots;
   q.hx_terms = t.hx_terms;
   q.hx_off = t.hx_off;
   q.ht_terms = t.ht_terms;
@@ -161,6 +163,7 @@ int dropin_tables(Problem& pb, const int* d_hx, const int* d_ht, TrackParams& p,
   p.n_hx_terms = (int)hxt.size();
   p.n_ht_terms = (int)htt.size();
   p.flat_eval = flat_eval_pays(hxo.data(), pb.N);  // the caller's own tables: their own walk
+  p.scr_slots = row_nonzeros_max(hxo.data(), pb.N);
   return GHC_OK;
 }
 

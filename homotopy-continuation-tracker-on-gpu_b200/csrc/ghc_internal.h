@@ -48,6 +48,18 @@ GHC_HD inline int term_col(uint64_t w) { return (int)(w >> 59); }
 // terms in that column; row-wise it runs as many as the longest row.  Above
 // 16 unknowns the kernels always walk rows (entry-wise code would be unrolled
 // N times).  hx_off: CSR offsets [N*N+1] of the compiled H_x terms.
+// The most structurally non-zero entries in one row of H_x: the row-wise walk stages each
+// row's non-zero entries in that many shared-memory slots.
+inline int row_nonzeros_max(const uint16_t* hx_off, int N) {
+  int most = 0;
+  for (int r = 0; r < N; ++r) {
+    int nz = 0;
+    for (int i = 0; i < N; ++i) nz += hx_off[r * N + i + 1] > hx_off[r * N + i];
+    if (nz > most) most = nz;
+  }
+  return most;
+}
+
 inline int flat_eval_pays(const uint16_t* hx_off, int N) {
   int longest = 0, per_entry = 0;
   for (int r = 0; r < N; ++r) {
@@ -72,6 +84,7 @@ struct TrackParams {
   int max_steps, max_corr, incr;
   int n_hx_terms, n_ht_terms;
   int flat_eval;              // walk H_x rows (flat_eval_pays() of the tables, or the autotuner's choice)
+  int scr_slots;              // row_nonzeros_max() of the tables
   int variant;                // compiled register-budget variant (0 or 1)
   int variant_f32, flat_eval_f32;  // the FP32 phase's choices in mixed precision
   const uint64_t* hx_terms;   // device
@@ -126,7 +139,7 @@ struct TrackParams {
 struct PolishParams {
   int kind, N, P, M, K;
   int n_hx_terms, n_ht_terms;
-  int flat_eval;
+  int flat_eval, scr_slots;
   const uint64_t* hx_terms;
   const uint16_t* hx_off;
   const uint64_t* ht_terms;

@@ -174,19 +174,21 @@ __device__ __forceinline__ cx<R> term_coef_value(uint64_t w, const cx<R>* ca) {
 // Flat (always above 16 unknowns, else when the problem's flat_eval is set):
 // the row's terms are walked as one list (CSR row r, column in the term word),
 // so a sub-warp spends max_r(terms of row r) iterations instead of
-// sum_i max_r(terms of entry (r, i)).  Each entry's sum is staged in the
-// sub-warp's scratch row scr[i][r] and read back into
-// registers; entries without terms are never written and stay zero from the
-// kernel's start.  Entry-wise: one loop per column, straight into registers.
-// Either way every entry is summed in table order, as in the oracle.
+// sum_i max_r(terms of entry (r, i)).  The k-th non-zero entry of the row is
+// staged in the sub-warp's scratch slot scr[k][r] (only as many slots as the
+// fullest row has non-zero entries) and read back into registers through the
+// lane's non-zero mask nz (entry i is in slot popc(nz & (2^i - 1))); every slot
+// below the row's count is rewritten by every evaluation.  Entry-wise: one loop
+// per column, straight into registers.  Either way every entry is summed in
+// table order, as in the oracle.
 template <int N>
 constexpr bool kFlatAlways = N > 16;
 
 template <typename R, int N, int W, int KIND>
 __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, const cx<R>* cb, const cx<R>* xs, int r,
                                          bool live, cx<R> (&A)[N], cx<R>& b, int which, bool flat,
-                                         unsigned char* scr) {
-  auto slot = [&](int i) -> cx<R>* { return view<R>(scr) + (i * W + r); };
+                                         unsigned char* scr, unsigned nz) {
+  auto slot = [&](int k) -> cx<R>* { return view<R>(scr) + (k * W + r); };
   if (!kFlatAlways<N> && !flat) {
 #pragma unroll
     for (int i = 0; i < N; ++i) {
@@ -203,22 +205,24 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
   } else {
     if (live) {
       const int len = tb.hx_off[r * N + N] - tb.hx_off[r * N];
-      int cur = -1;
+      int cur = -1, k = -1;
       cx<R> acc = mk(R(0), R(0));
-      for (int k = 0; k < len; ++k) {
-        const uint64_t w = tb.hx_terms[k * N + r];
+      for (int q = 0; q < len; ++q) {
+        const uint64_t w = tb.hx_terms[q * N + r];
         const int i = term_col(w);
         if (i != cur) {
-          if (cur >= 0) *slot(cur) = acc;
+          if (cur >= 0) *slot(k) = acc;
+          ++k;
           acc = mk(R(0), R(0));
           cur = i;
         }
         acc = acc_term(acc, term_coef_value<R, KIND>(w, ca), w, xs);
       }
-      if (cur >= 0) *slot(cur) = acc;
+      if (cur >= 0) *slot(k) = acc;
     }
 #pragma unroll
-    for (int i = 0; i < N; ++i) A[i] = live ? *slot(i) : mk(R(0), R(0));
+    for (int i = 0; i < N; ++i)
+      A[i] = ((nz >> i) & 1u) ? *slot(__popc(nz & ((1u << i) - 1u))) : mk(R(0), R(0));
   }
   cx<R> h = mk(R(0), R(0));
   if (live) {
@@ -432,8 +436,19 @@ struct SubMem {
   unsigned char* sx;     // two pivot rows + rhs [2][N+1]
   unsigned char* sol;    // solution [N]
   unsigned char* state;  // per lane: RK base point x0 [W], RK accumulator [W]
-  unsigned char* scr;    // H_x row scratch [N][W], null unless the evaluation is flat
+  unsigned char* scr;    // H_x row scratch [slots][W], null unless the evaluation is flat
+  unsigned nz;           // this lane's row: bit i set when H_x entry (row, i) has terms
 };
+
+// bit i set when row r of H_x has terms in column i (0 for lanes beyond the rows)
+template <int N>
+__device__ __forceinline__ unsigned row_mask(const uint16_t* hx_off, int r) {
+  unsigned m = 0u;
+  if (r < N)
+    for (int i = 0; i < N; ++i)
+      if (hx_off[r * N + i + 1] > hx_off[r * N + i]) m |= 1u << i;
+  return m;
+}
 
 // one evaluation + solve in precision R; returns this lane's solution component
 template <typename R, int N, int W, int KIND>
@@ -441,7 +456,7 @@ __device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, 
   cx<R> A[N];
   cx<R> b;
   eval_row<R, N, W, KIND>(tb, view<R>(sm.coefA), view<R>(sm.coefB), view<R>(sm.xs), l, l < N, A, b, which,
-                          sm.scr != nullptr, sm.scr);
+                          sm.scr != nullptr, sm.scr, sm.nz);
   lu_solve<R, N, W>(A, b, l, view<R>(sm.sx), view<R>(sm.sol));
   const cx<R> k = (l < N) ? view<R>(sm.sol)[l] : mk(R(0), R(0));
   return k;
@@ -471,9 +486,9 @@ __host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
   return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(N * N + 1 + N + 1));
 }
 // per sub-warp, in complex values of esz bytes: coefficient buffers [2 Mc], track [N+1],
-// two pivot rows [2 (N+1)], solution [N], lane state [2 W], scratch row [N W] when flat
-__host__ __device__ inline size_t sub_bytes(int N, int Mc, int W, bool flat, int esz) {
-  return align16((size_t)esz * (2 * (size_t)Mc + 3 * (N + 1) + N + 2 * W + (flat ? N * W : 0)));
+// two pivot rows [2 (N+1)], solution [N], lane state [2 W], scratch slots [slots W] (flat)
+__host__ __device__ inline size_t sub_bytes(int N, int Mc, int W, int slots, int esz) {
+  return align16((size_t)esz * (2 * (size_t)Mc + 3 * (N + 1) + N + 2 * W + (size_t)slots * W));
 }
 template <typename R>
 __device__ __forceinline__ SubMem sub_layout(unsigned char* base, int N, int Mc, int W, bool flat) {
@@ -487,13 +502,6 @@ __device__ __forceinline__ SubMem sub_layout(unsigned char* base, int N, int Mc,
   sm.state = sm.sol + e * N;
   sm.scr = flat ? sm.state + 2 * e * W : nullptr;
   return sm;
-}
-
-// zero this lane's slots of the scratch row (lane l owns slots i*W + l)
-template <typename R, int N, int W>
-__device__ __forceinline__ void zero_scratch(unsigned char* scr, int l) {
-#pragma unroll
-  for (int i = 0; i < N; ++i) view<R>(scr)[i * W + l] = mk(R(0), R(0));
 }
 
 // complex entry idx of an array of doubles (f64) or floats, in precision R
@@ -574,13 +582,13 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const bool flat = kFlatAlways<N> || p.flat_eval;
-  const SubMem sm = sub_layout<R>(smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) +
-                                      (size_t)g * sub_bytes(N, Mc, W, flat, (int)sizeof(cx<R>)),
-                                  N, Mc, W, flat);
+  SubMem sm = sub_layout<R>(smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) +
+                                (size_t)g * sub_bytes(N, Mc, W, flat ? p.scr_slots : 0, (int)sizeof(cx<R>)),
+                            N, Mc, W, flat);
+  sm.nz = row_mask<N>(tb.hx_off, l);
   // this lane's RK base point x0 and accumulator sols live in shared memory (register relief)
   cx<R>& x0 = view<R>(sm.state)[l];
   cx<R>& sols = view<R>(sm.state)[W + l];
-  if (flat) zero_scratch<R, N, W>(sm.scr, l);
 
   const int subs_per_cta = blockDim.x / W;
   const long long n_sw = (long long)gridDim.x * subs_per_cta;
@@ -776,9 +784,10 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const bool flat = kFlatAlways<N> || p.flat_eval;
-  const SubMem sm = sub_layout<double>(
-      smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, W, flat, 16), N, Mc, W, flat);
-  if (flat) zero_scratch<double, N, W>(sm.scr, l);
+  SubMem sm = sub_layout<double>(
+      smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, W, flat ? p.scr_slots : 0, 16),
+      N, Mc, W, flat);
+  sm.nz = row_mask<N>(tb.hx_off, l);
   const int subs_per_cta = blockDim.x / W;
   const int leader = lane - l;
   for (long long item0 = (long long)blockIdx.x * subs_per_cta; item0 < p.n_items;
@@ -811,7 +820,7 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
     cx<double> A[N];
     cx<double> h;
     eval_row<double, N, W, KIND>(tb, view<double>(sm.coefA), view<double>(sm.coefB), view<double>(sm.xs), l, l < N, A,
-                                 h, 0, flat, sm.scr);
+                                 h, 0, flat, sm.scr, sm.nz);
     const double s = tree_sum<double, N, W>(l < N ? c_abs2(h) : 0.0);
     const double s0 = __shfl_sync(kFull, s, leader);
     if (valid) {

@@ -16,9 +16,9 @@ int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
   auto kern = dev::track_kernel<R, N, W, KIND, V>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
-  const bool flat = dev::kFlatAlways<N> || p.flat_eval;
+  const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
   const size_t smem =
-      dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, flat, 2 * (int)sizeof(R));
+      dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, slots, 2 * (int)sizeof(R));
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return -20;
   int occ = 0;
@@ -42,8 +42,8 @@ int launch_polish_t(const PolishParams& p, cudaStream_t s) {
   auto kern = dev::polish_kernel<N, W, KIND>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
-  const bool flat = dev::kFlatAlways<N> || p.flat_eval;
-  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, flat, 16);
+  const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
+  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, slots, 16);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -20;
   long long grid = (p.n_items + subs - 1) / subs;
   if (grid > 65535LL * 16) grid = 65535LL * 16;

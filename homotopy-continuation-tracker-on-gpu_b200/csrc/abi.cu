@@ -541,25 +541,37 @@ int ghc_autotune(ghc_problem* h, const ghc_track_args* a, void* stream, ghc_tune
     set_error("unknown precision mode");
     return GHC_ERR_ARG;
   }
-  std::vector<std::pair<int, int>> cand;
-  for (int v = 0; v < 2; ++v) {
-    if (pb.N > 16) {
-      cand.push_back({v, 1});
-    } else {
-      cand.push_back({v, 1});
-      cand.push_back({v, 0});
-    }
-  }
+  struct Cand {
+    int v64, v32, flat;
+  };
+  std::vector<Cand> cand;
+  const bool mixed = prec == GHC_PREC_MIXED;
+  for (int f = 1; f >= (pb.N > 16 ? 1 : 0); --f)
+    for (int v = 0; v < 2; ++v)
+      for (int w = 0; w < (mixed ? 2 : 1); ++w) cand.push_back({v, mixed ? w : v, f});
   const int keep_v[2] = {pb.tune_variant[0], pb.tune_variant[1]};
   const int keep_f[2] = {pb.tune_flat[0], pb.tune_flat[1]};
+  auto apply = [&](const Cand& c) {
+    if (prec == GHC_PREC_FP32) {
+      pb.tune_variant[1] = c.v64;
+      pb.tune_flat[1] = c.flat;
+    } else {
+      pb.tune_variant[0] = c.v64;
+      pb.tune_flat[0] = c.flat;
+      if (mixed) {
+        pb.tune_variant[1] = c.v32;
+        pb.tune_flat[1] = c.flat;
+      }
+    }
+  };
   cudaStream_t st = (cudaStream_t)stream;
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return cuda_fail("autotune events");
   double best_ms = HUGE_VAL;
   int rc = GHC_OK;
-  std::pair<int, int> win = cand[0];
+  Cand win = cand[0];
   for (const auto& c : cand) {
-    ghc_set_tuning(h, prec, c.first, c.second);
+    apply(c);
     for (int rep = 0; rep < 2 && !rc; ++rep) {  // the first run warms up (kernel attributes, caches)
       cudaEventRecord(e0, st);
       rc = ghc_track(h, a, stream);
@@ -586,9 +598,10 @@ int ghc_autotune(ghc_problem* h, const ghc_track_args* a, void* stream, ghc_tune
     pb.tune_flat[1] = keep_f[1];
     return rc;
   }
-  ghc_set_tuning(h, prec, win.first, win.second);
-  best->variant = win.first;
-  best->flat = win.second;
+  apply(win);
+  best->variant = win.v64;
+  best->variant_f32 = mixed ? win.v32 : (prec == GHC_PREC_FP32 ? win.v64 : pb.tune_variant[1]);
+  best->flat = win.flat;
   best->ms = best_ms;
   best->candidates = (int)cand.size();
   return GHC_OK;

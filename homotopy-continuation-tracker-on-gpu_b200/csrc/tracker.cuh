@@ -520,15 +520,16 @@ __device__ __forceinline__ cx<R> load_cx(const void* base, bool f64, long long i
 // compiled variants per size and precision; the autotuner (ghc_autotune) picks
 // one per problem.  Variant 0 is the best of B200 sweeps over the shipped
 // problems (FP64 N = 3 at 6 -- at 8 the 64 registers spill --, N = 6 and
-// N = 12 at 4); variant 1 trades registers for one more CTA per SM (N = 12:
+// N = 12 at 4); variant 1 trades registers for more CTAs per SM (N = 12:
 // better for the uncalibrated trifocal problem, worse for the generalized
-// 3-view problem, which have the same size).
+// 3-view problem, which have the same size; N = 30: FP64 342 vs 308 hyp/s at
+// 3 instead of 2 CTAs, FP32 488 vs 450 at 5 instead of 3).
 template <int N, typename R, int V>
 constexpr int track_min_blocks() {
   return V == 0 ? (sizeof(R) == 8 ? (N <= 4 ? 6 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
                                   : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 3))
                 : (sizeof(R) == 8 ? (N <= 4 ? 8 : N <= 12 ? 5 : N <= 18 ? 4 : 3)
-                                  : (N <= 8 ? 6 : N <= 12 ? 5 : N <= 18 ? 3 : 2));
+                                  : (N <= 8 ? 10 : N <= 12 ? 8 : 5));
 }
 
 __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64_t* g_hx, const uint16_t* g_hxo,

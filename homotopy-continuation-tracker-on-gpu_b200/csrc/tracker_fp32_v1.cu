@@ -1,4 +1,4 @@
-// tracker_fp32_v1.cu -- FP32 tracker, register-budget variant 1.
+// tracker_fp32_v1.cu -- FP32 tracker, register-budget variant 1 (more CTAs per SM).
 #include "tracker_launch.cuh"
 
 namespace ghc {

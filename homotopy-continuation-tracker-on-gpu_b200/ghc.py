@@ -44,7 +44,8 @@ class Counts(ctypes.Structure):
 
 
 class TuneChoice(ctypes.Structure):
-    _fields_ = [("variant", _I32), ("flat", _I32), ("ms", ctypes.c_double), ("candidates", _I32)]
+    _fields_ = [("variant", _I32), ("flat", _I32), ("ms", ctypes.c_double), ("candidates", _I32),
+                ("variant_f32", _I32)]
 
 
 class TrackArgs(ctypes.Structure):
@@ -230,7 +231,8 @@ def autotune(pb, ws, d_start_sols, **kw):
     a = _track_args(ws, d_start_sols, **kw)
     out = TuneChoice()
     _check(ghc_autotune(pb.h, ctypes.byref(a), _stream(), ctypes.byref(out)), "ghc_autotune")
-    return dict(variant=out.variant, flat=out.flat, ms=out.ms, candidates=out.candidates)
+    return dict(variant=out.variant, flat=out.flat, ms=out.ms, candidates=out.candidates,
+                variant_f32=out.variant_f32)
 
 
 def set_tuning(pb, precision, variant, flat=-1):

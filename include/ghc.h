@@ -173,13 +173,15 @@ int ghc_track_noalloc(const ghc_problem* pb, const ghc_track_args* args, void* s
  * ghc_autotune runs the caller's sample batch (`sample`, exactly as for
  * ghc_track, outputs overwritten) once per candidate after a warm-up, times it
  * with CUDA events on `stream`, keeps the fastest in the handle for
- * sample->precision (mixed: both phases) and returns it.  It synchronises
+ * sample->precision (mixed: both phases, their variants chosen independently)
+ * and returns it.  It synchronises
  * `stream`; do not run it while the handle is tracking elsewhere.
  * ------------------------------------------------------------------------- */
 typedef struct {
   int32_t variant, flat;
   double ms;                  /* the sample's time with this choice */
   int32_t candidates;         /* how many were timed */
+  int32_t variant_f32;        /* GHC_PREC_MIXED: the FP32 phase's variant (the FP64 phase's is `variant`) */
 } ghc_tune_choice;
 
 int ghc_autotune(ghc_problem* pb, const ghc_track_args* sample, void* stream, ghc_tune_choice* best);

@@ -64,3 +64,14 @@ def test_autotune_keeps_a_candidate():
     assert torch.equal(ws.endpoints, ref.endpoints)  # the sample's outputs are a regular run's
     again, _ = _run(pb, ob, tg, ghc.PREC_FP64)
     assert torch.equal(again.endpoints, ref.endpoints)
+
+
+def test_mixed_autotune_chooses_each_phase():
+    """Mixed precision tunes the FP64 and FP32 phases' variants independently (2 x 2 x 2 walks)."""
+    pb, ob, tg = _inputs("generalized_3views_4pts", H=8)
+    ref, _ = _run(pb, ob, tg, ghc.PREC_MIXED, (0, -1))
+    ws, choice = _run(pb, ob, tg, ghc.PREC_MIXED, "auto")
+    assert choice["candidates"] == 8
+    assert ghc.get_tuning(pb, ghc.PREC_FP64) == (choice["variant"], choice["flat"])
+    assert ghc.get_tuning(pb, ghc.PREC_FP32) == (choice["variant_f32"], choice["flat"])
+    assert torch.equal(ws.endpoints, ref.endpoints)

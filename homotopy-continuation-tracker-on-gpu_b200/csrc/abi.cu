@@ -698,31 +698,55 @@ int ghc_solve_host(const ghc_problem* h, int32_t precision, int64_t n_hyp, const
   const int N = pb.N, P1 = pb.P + 1;
   const size_t rs = fp32 ? sizeof(float) : sizeof(double);
   const long long nhx = 2LL * (pb.M + 1) * (pb.K + 1), nht = 2LL * (pb.M + 1) * pb.K;
-  TmpFree tmp;
-  auto dmalloc = [&](size_t bytes) -> void* {
-    void* p = nullptr;
-    if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
-    tmp.v.push_back(p);
-    return p;
-  };
-  void* d_start = dmalloc(2 * (size_t)pb.paths * N * rs);
-  double* d_ps = (double*)dmalloc(2 * (size_t)P1 * sizeof(double));
-  double* d_tg = (double*)dmalloc(2 * (size_t)P1 * n_hyp * sizeof(double));
-  double* d_pd = (double*)dmalloc(2 * (size_t)P1 * n_hyp * sizeof(double));
-  double* d_hx = pb.kind == KIND_P2C ? (double*)dmalloc(nhx * n_hyp * sizeof(double)) : nullptr;
-  double* d_ht = pb.kind == KIND_P2C ? (double*)dmalloc(std::max(nht, 1LL) * n_hyp * sizeof(double)) : nullptr;
-  void* d_ep = dmalloc(2 * (size_t)n * N * rs);
-  uint8_t* d_flags = (uint8_t*)dmalloc(3 * (size_t)n);
-  int32_t* d_steps = (int32_t*)dmalloc((size_t)n * 8 + 16);  // steps, corrector iterations
-  double* d_tdt = (double*)dmalloc((size_t)n * 16 + 16);       // t_end, dt_end
-  if (!d_start || !d_ps || !d_tg || !d_pd || !d_ep || !d_flags || !d_steps || !d_tdt ||
-      (pb.kind == KIND_P2C && (!d_hx || !d_ht)))
-    return cuda_fail("allocation");
+  // all device buffers from one grow-only arena of the handle (no allocation once it is large
+  // enough), work on the handle's own non-blocking stream
+  const size_t sz[10] = {2 * (size_t)pb.paths * N * rs,
+                         2 * (size_t)P1 * sizeof(double),
+                         2 * (size_t)P1 * n_hyp * sizeof(double),
+                         2 * (size_t)P1 * n_hyp * sizeof(double),
+                         pb.kind == KIND_P2C ? nhx * n_hyp * sizeof(double) : 0,
+                         pb.kind == KIND_P2C ? std::max(nht, 1LL) * n_hyp * sizeof(double) : 0,
+                         2 * (size_t)n * N * rs,
+                         3 * (size_t)n,
+                         (size_t)n * 8,
+                         (size_t)n * 16};
+  size_t total = 0;
+  for (size_t b : sz) total += (b + 255) & ~(size_t)255;
+  if (total > pb.dev.solve_bytes) {
+    cudaFree(pb.dev.solve_arena);
+    pb.dev.solve_arena = nullptr;
+    pb.dev.solve_bytes = 0;
+    if (cudaMalloc(&pb.dev.solve_arena, total) != cudaSuccess) return cuda_fail("allocation");
+    pb.dev.solve_bytes = total;
+  }
+  if (!pb.dev.solve_stream) {
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return cuda_fail("stream");
+    pb.dev.solve_stream = s;
+  }
+  void* buf[10];
+  {
+    char* q = (char*)pb.dev.solve_arena;
+    for (int k = 0; k < 10; ++k) {
+      buf[k] = sz[k] ? q : nullptr;
+      q += (sz[k] + 255) & ~(size_t)255;
+    }
+  }
+  void* d_start = buf[0];
+  double* d_ps = (double*)buf[1];
+  double* d_tg = (double*)buf[2];
+  double* d_pd = (double*)buf[3];
+  double* d_hx = (double*)buf[4];
+  double* d_ht = (double*)buf[5];
+  void* d_ep = buf[6];
+  uint8_t* d_flags = (uint8_t*)buf[7];
+  int32_t* d_steps = (int32_t*)buf[8];  // steps, corrector iterations
+  double* d_tdt = (double*)buf[9];      // t_end, dt_end
   if (pb.kind == KIND_P2C && !pb.has_terms) {
     set_error("problem has no coefficient expressions (p2c_terms.txt)");
     return GHC_ERR_NOP2C;
   }
-  cudaStream_t st = 0;
+  cudaStream_t st = (cudaStream_t)pb.dev.solve_stream;
   cudaEvent_t ev[4];
   for (auto& e : ev) cudaEventCreate(&e);
   std::vector<float> sf;

@@ -101,6 +101,8 @@ Problem::~Problem() {
     cudaFree(dev.t_fac);
     cudaFree(dev.k_off);
     cudaFree(dev.scratch);
+    cudaFree(dev.solve_arena);
+    if (dev.solve_stream) cudaStreamDestroy((cudaStream_t)dev.solve_stream);
     cudaFree(dev.counter);
     cudaSetDevice(cur);
   }

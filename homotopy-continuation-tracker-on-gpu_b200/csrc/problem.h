@@ -31,6 +31,10 @@ struct DeviceTables {
   // drop-in scratch (grow-only)
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
+  // ghc_solve_host: grow-only device arena and the handle's own non-blocking stream
+  void* solve_arena = nullptr;
+  size_t solve_bytes = 0;
+  void* solve_stream = nullptr;
   int* counter = nullptr;
 };
 

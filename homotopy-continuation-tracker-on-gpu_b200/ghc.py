@@ -310,18 +310,30 @@ def count_results_device(ws, N, imag_tol=1e-4, dup_tol=1e-4, want_class=False, o
     return counts, cls
 
 
-def solve_host(pb, precision=PREC_FP64, targets=None, t_switch=0.9, polish_iters=0):
-    """One-call host solve (host buffers in and out, copies included)."""
-    n_hyp = 1 if targets is None else np.asarray(targets).shape[0]
+def solve_outputs(pb, n_hyp):
+    """Host output arrays for solve_host (reusable across calls of the same size)."""
     n = n_hyp * pb.paths
-    ep = np.zeros((n, pb.N, 2))
-    st = np.zeros(n, np.uint8)
-    cv = np.zeros(n, np.uint8)
-    nf = np.zeros(n, np.uint8)
-    steps = np.zeros(n, np.int32)
-    ms = np.zeros(3)
-    tg = None if targets is None else _cx_np(targets)
+    return dict(endpoints=np.zeros((n, pb.N), np.complex128), status=np.zeros(n, np.uint8),
+                conv=np.zeros(n, np.uint8), inf=np.zeros(n, np.uint8), steps=np.zeros(n, np.int32),
+                ms=np.zeros(3))
+
+
+def solve_host(pb, precision=PREC_FP64, targets=None, t_switch=0.9, polish_iters=0, out=None):
+    """One-call host solve (host buffers in and out, copies included).
+
+    targets: [n_hyp, P+1] complex (None: the problem's target, n_hyp = 1).  out: arrays from
+    solve_outputs() to fill in place (fresh ones otherwise).  Returns the dict of arrays;
+    endpoints [n_hyp * paths, N] complex128 is written directly by the library."""
+    n_hyp = 1 if targets is None else np.asarray(targets).shape[0]
+    o = out if out is not None else solve_outputs(pb, n_hyp)
+    if o["endpoints"].shape != (n_hyp * pb.paths, pb.N) or o["endpoints"].dtype != np.complex128:
+        raise GhcError("solve_host: output arrays of the wrong size")
+    tg = None
+    if targets is not None:
+        tg = np.asarray(targets)
+        if tg.dtype != np.complex128 or not tg.flags.c_contiguous:
+            tg = np.ascontiguousarray(tg, dtype=np.complex128)
     _check(ghc_solve_host(pb.h, precision, n_hyp, None if tg is None else tg.ctypes.data, t_switch, polish_iters,
-                          ep.ctypes.data, st.ctypes.data, cv.ctypes.data, nf.ctypes.data, steps.ctypes.data,
-                          ms.ctypes.data), "ghc_solve_host")
-    return dict(endpoints=_np_cx(ep), status=st, conv=cv, inf=nf, steps=steps, ms=ms)
+                          o["endpoints"].ctypes.data, o["status"].ctypes.data, o["conv"].ctypes.data,
+                          o["inf"].ctypes.data, o["steps"].ctypes.data, o["ms"].ctypes.data), "ghc_solve_host")
+    return o

@@ -248,6 +248,8 @@ double ghc_kernel_HC_Solver_PH_z(const ghc_problem* pb, void* stream, int max_st
  * h_targets: [n_hyp][P+1] complex (NULL: the problem's target_params.txt, n_hyp = 1).
  * h_endpoints: [n_hyp*paths][N] complex double.  h_status, h_steps optional.
  * h_ms (optional): [0] H2D, [1] P2C + track + polish, [2] D2H, milliseconds.
+ * Device buffers come from a grow-only arena of the handle and the work runs on the
+ * handle's own stream, so calls on one handle must not overlap.
  * ------------------------------------------------------------------------- */
 int ghc_solve_host(const ghc_problem* pb, int32_t precision, int64_t n_hyp, const double* h_targets,
                    double t_switch, int32_t polish_iters, double* h_endpoints, uint8_t* h_status, uint8_t* h_conv,

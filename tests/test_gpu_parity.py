@@ -233,6 +233,23 @@ def test_solve_host_end_to_end(name, prec):
     assert np.array_equal(out["endpoints"], to_cx(ws.endpoints))
 
 
+def test_solve_host_arena_and_reused_outputs():
+    """Calls of different sizes on one handle (the device arena grows, then is reused) give the
+    same results as fresh calls, also when the output arrays are reused."""
+    pb, ob, tg = inputs("generalized_3views_4pts", n_hyp=5, seed=21)
+    small1 = ghc.solve_host(pb, ghc.PREC_FP64, targets=tg[:2])
+    large = ghc.solve_host(pb, ghc.PREC_FP64, targets=tg)
+    out = ghc.solve_outputs(pb, 2)
+    small2 = ghc.solve_host(pb, ghc.PREC_FP64, targets=tg[:2], out=out)
+    small3 = ghc.solve_host(pb, ghc.PREC_FP64, targets=tg[:2], out=out)
+    assert small3 is out
+    n = 2 * pb.paths
+    for k in ("endpoints", "conv", "status", "steps"):
+        assert np.array_equal(small1[k], small3[k]) and np.array_equal(large[k][:n], small1[k])
+    with pytest.raises(ghc.GhcError):
+        ghc.solve_host(pb, ghc.PREC_FP64, targets=tg, out=out)
+
+
 @pytest.mark.parametrize("name,prec", [("P3P", "f"), ("uncalibrated_trifocal_rel_pos_CY", "f"),
                                        ("generalized_3views_4pts", "d"), ("trifocal_2op1p_30x30", "f"),
                                        ("trifocal_2op1p_30x30", "d")])

@@ -167,6 +167,39 @@ def ref_p2c(pb, start, target, precision="d"):
     return (hx[0::2] + 1j * hx[1::2]).astype(np.complex128), (ht[0::2] + 1j * ht[1::2]).astype(np.complex128)
 
 
+_REF_EVAL = None
+
+
+def ref_eval_available(name):
+    f = os.path.join(HERE, "_ref", "eval_problems.txt")
+    return os.path.exists(os.path.join(HERE, "_ref", "libeval_ref.so")) and os.path.exists(f) and \
+        name in open(f).read().split()
+
+
+def ref_eval(pb, x, c, cp):
+    """The reference's own evaluators (dev-eval-indxing-<p>.cuh, compiled by oracle/ref/build_ref.py)
+    at track x [N] with coefficients c_k(t), c'_k(t) [M+1] (PH: p(t), p1 - p0 [P+1]):
+    returns (Hx [N, N], -H_t [N], H [N])."""
+    global _REF_EVAL
+    if _REF_EVAL is None:
+        _REF_EVAL = ctypes.CDLL(os.path.join(HERE, "_ref", "libeval_ref.so"))
+    fn = getattr(_REF_EVAL, "ref_eval_%s" % pb.name)
+    p = ctypes.c_void_p
+    fn.argtypes = [p] * 8
+    N = pb.N
+    xs = _cx(np.append(np.asarray(x, dtype=np.complex128), 1.0), np.float64)
+    cc, ccp = _cx(c, np.float64), _cx(cp, np.float64)
+    hx_idx = np.ascontiguousarray(pb.hx_idx, dtype=np.int32)
+    ht_idx = np.ascontiguousarray(pb.ht_idx, dtype=np.int32)
+    Hx = np.zeros((N, N, 2))
+    Ht = np.zeros((N, 2))
+    H = np.zeros((N, 2))
+    fn(xs.ctypes.data, cc.ctypes.data, ccp.ctypes.data, hx_idx.ctypes.data, ht_idx.ctypes.data, Hx.ctypes.data,
+       Ht.ctypes.data, H.ctypes.data)
+    cx = lambda a: a[..., 0] + 1j * a[..., 1]  # noqa: E731
+    return cx(Hx), cx(Ht), cx(H)
+
+
 # ----------------------------------------------------------------------------
 # tracker (ctypes)
 # ----------------------------------------------------------------------------

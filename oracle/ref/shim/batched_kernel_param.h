@@ -1,0 +1,1 @@
+/* empty stand-in (oracle/_ref build only) */

@@ -1,7 +1,8 @@
 /*
  * Stand-in for MAGMA's magma_v2.h, just enough for the reference's generated
- * P2C coefficient builders (GPU-HC/magmaHC/PHC_Coeffs/p2c-*.h) to compile on
- * the host.  TEST INFRASTRUCTURE ONLY (oracle/_ref).  The complex scalar type
+ * P2C coefficient builders (GPU-HC/magmaHC/PHC_Coeffs/p2c-*.h) and its
+ * evaluator templates (GPU-HC/magmaHC/gpu-idx-evals/dev-eval-indxing-*.cuh) to
+ * compile on the host.  TEST INFRASTRUCTURE ONLY (oracle/_ref).  The complex scalar type
  * is chosen with REF_REAL (double by default) so the reference's coefficient
  * expressions can be evaluated in the tracker's precision.
  */
@@ -36,6 +37,8 @@ template <class S, class = typename std::enable_if<std::is_arithmetic<S>::value>
 inline ref_cx operator-(S s, ref_cx a) { return ref_cx((REF_REAL)s - a.x, -a.y); }
 template <class S, class = typename std::enable_if<std::is_arithmetic<S>::value>::type>
 inline ref_cx operator-(ref_cx a, S s) { return ref_cx(a.x - (REF_REAL)s, a.y); }
+inline ref_cx& operator+=(ref_cx& a, ref_cx b) { a.x += b.x; a.y += b.y; return a; }
+inline ref_cx& operator-=(ref_cx& a, ref_cx b) { a.x -= b.x; a.y -= b.y; return a; }
 typedef ref_cx magmaFloatComplex;
 #define MAGMA_C_MAKE(a, b) ref_cx((REF_REAL)(a), (REF_REAL)(b))
 #define MAGMA_C_ONE ref_cx(1, 0)

@@ -75,6 +75,36 @@ def test_p2c_matches_reference_builder(name):
 
 
 @pytest.mark.parametrize("name", ALL_PROBLEMS)
+def test_evaluators_match_reference_evaluators(name):
+    """The oracle's H_x, H_t and H equal those of the reference's own evaluator templates
+    (GPU-HC/magmaHC/gpu-idx-evals/dev-eval-indxing-<p>.cuh, compiled from the reference tree by
+    oracle/ref/build_ref.py) at random complex tracks and times, to rounding."""
+    if not O.ref_eval_available(name):
+        pytest.skip("oracle/_ref evaluators not built (needs the reference tree)")
+    pb = O.Problem(name)
+    rng = np.random.default_rng(7)
+    target = np.append(rng.normal(size=pb.P) + 1j * rng.normal(size=pb.P), 1.0)
+    if pb.kind == O.P2C:
+        hx, ht = coefs(pb, target)
+        K, Mc = pb.K, pb.M + 1
+    for _ in range(3):
+        t = rng.uniform(0, 1)
+        x = rng.normal(size=pb.N) + 1j * rng.normal(size=pb.N)
+        if pb.kind == O.P2C:
+            c = np.array([sum(hx[k * (K + 1) + e] * t ** e for e in range(K + 1)) for k in range(Mc)])
+            cp = np.array([sum(ht[k * K + e] * t ** e for e in range(K)) for k in range(Mc)])
+            H, Ht, Hx = O.eval_system(pb, x, t, hx=hx, ht=ht)
+        else:
+            c = target * t + pb.start_params * (1 - t)
+            c[-1] = 1.0
+            cp = target - pb.start_params
+            H, Ht, Hx = O.eval_system(pb, x, t, p_start=pb.start_params, p_target=target)
+        rHx, rHt, rH = O.ref_eval(pb, x, c, cp)
+        for mine, ref in ((Hx, rHx), (Ht, -rHt), (H, rH)):  # the reference returns -H_t
+            assert np.abs(mine - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("name", ALL_PROBLEMS)
 def test_start_solutions_solve_start_system(name):
     pb = O.Problem(name)
     if pb.kind == O.P2C:

@@ -603,6 +603,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
   long long hyp = 0;
   cx<R> x = mk(R(0), R(0));
   R t0 = 0, dt = 0, t_step = 0, half = 0, dt_pre = 0;
+  R coef_t = R(-1);  // the t at which this sub-warp's coefficient buffers hold c_k(t) (-1: none)
   bool end_zone = false, success = false, inf = false, finished = false;
   int nsucc = 0, step = 0, ncorr = 0, phase = 0, cit = 0, nfail = 0;
   const R dt_init = (KIND == KIND_PH) ? R(0.01) : R(0.05);
@@ -644,6 +645,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
     x0 = x;
     sols = x;
     t0 = p.t_in ? (R)p.t_in[it] : R(0);
+    coef_t = R(-1);  // a new path may belong to another hypothesis
     dt = p.dt_in ? (R)p.dt_in[it] : dt_init;
     dt_pre = dt;
     step = p.resume ? p.steps[it] : 0;
@@ -662,8 +664,13 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
     const bool served = alive && !finished;
     const bool rk = served && phase < 4;
     const bool corr = served && phase == 4;
-    // ---------------- coefficients: every RK stage at its t; the corrector reuses stage 4's
-    if (rk) coef_eval<R, W, KIND>(p, sm, hyp, t0, l);
+    // ---------------- coefficients c_k(t) of the RK stage; the corrector reuses the last stage's
+    // (RK stages 2 and 3 share t + dt/2, and after an accepted step the next step starts at the t
+    // of the last stage, whose coefficients are still in the buffers: evaluate only on a new t)
+    if (rk && t0 != coef_t) {
+      coef_eval<R, W, KIND>(p, sm, hyp, t0, l);
+      coef_t = t0;
+    }
     // ---------------- one evaluate-and-solve per sub-warp (predictor: -H_t, corrector: H)
     write_track<R, N>(sm, l, x);
     __syncwarp(kFull);

@@ -102,3 +102,19 @@ def test_cayley_is_a_scaled_rotation():
         r = rng.normal(size=3)
         R = scenes.cayley(r) / (1 + r @ r)
         assert np.allclose(R @ R.T, np.eye(3), atol=1e-12) and abs(np.linalg.det(R) - 1) < 1e-12
+
+
+def test_quadratic_total_degree_generator(tmp_path):
+    """gen/make_quadratic_td.py writes a folder both readers accept, whose start solutions solve the
+    start system, and whose paths the oracle tracks to solutions of the target system."""
+    import make_quadratic_td
+    make_quadratic_td.write(str(tmp_path), 5, paths=12, seed=1)
+    ob = O.Problem("QTD_5", root=str(tmp_path))
+    assert ob.paths == 12 and ob.N == 5
+    hx, ht = O.p2c_tables(ob.terms, ob.start_params, ob.target_params)
+    hx0, ht0 = O.p2c_tables(ob.terms, ob.start_params, ob.start_params)
+    for x in ob.start_sols:
+        H, _, _ = O.eval_system(ob, x, 0.0, hx=hx0, ht=ht0)
+        assert np.abs(H).max() < 1e-12
+    r = O.track(ob, ob.start_sols, hx=hx, ht=ht, polish_iters=2)
+    assert (r["resid"][r["conv"] == 1] < 1e-10).all() and r["conv"].mean() > 0.9

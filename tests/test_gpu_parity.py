@@ -109,6 +109,36 @@ def test_fp32_bit_exact_vs_oracle(name):
     compare(ws, r)
 
 
+SYNTH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "problems")
+
+
+@pytest.mark.parametrize("N", [4, 11, 16, 18])
+@pytest.mark.parametrize("prec", [ghc.PREC_FP64, ghc.PREC_FP32, ghc.PREC_MIXED])
+def test_synthetic_sizes_bit_exact(N, prec):
+    """The sizes no shipped problem has (coupled quadratics generated by gen/make_quadratic_td.py):
+    every compiled P2C size runs and matches the oracle bit for bit, with both H_x walks."""
+    name = "QTD_%d" % N
+    pb, ob = ghc.Problem(name, root=SYNTH), O.Problem(name, root=SYNTH)
+    rng = np.random.default_rng(N)
+    tg = np.array([ob.target_params, np.append(ob.target_params[:-1] + 0.1 * rng.normal(size=ob.P), 1.0)])
+    hx = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[0] for t in tg])
+    ht = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[1] for t in tg])
+    rt = torch.float32 if prec == ghc.PREC_FP32 else torch.float64
+    if prec == ghc.PREC_FP32:
+        r = O.track(ob, ob.start_sols.astype(np.complex64), hx=hx.astype(np.complex64), ht=ht.astype(np.complex64),
+                    precision="f", nthreads=NCPU)
+    else:
+        r = O.track(ob, ob.start_sols, hx=hx, ht=ht, precision="mixed" if prec == ghc.PREC_MIXED else "d",
+                    t_switch=0.9, nthreads=NCPU)
+    for flat in ([1] if N > 16 else [0, 1]):
+        ghc.set_tuning(pb, prec, 0, flat)
+        ws = ghc.Workspace(pb, 2, prec)
+        ghc.track(pb, ws, cx_t(ob.start_sols, rt), d_coef_hx=cx_t(hx), d_coef_ht=cx_t(ht), t_switch=0.9)
+        torch.cuda.synchronize()
+        compare(ws, r)
+    assert r["conv"].mean() > 0.9
+
+
 @pytest.mark.parametrize("name,robust,t_switch", [("P3P", False, 0.9), ("generalized_3views_4pts", False, 0.9),
                                                   ("generalized_3views_4pts", True, 0.5),
                                                   ("uncalibrated_trifocal_rel_pos_CY", False, 0.9),

@@ -238,8 +238,10 @@ def config_g3v4_mono(args, torch):
     step = dict(step=dict(corr_tol2=1e-12, first_tol2=1e-2, dt_max=0.05), max_corr=3, max_steps=2000)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     for name, prec in (("fp64", ghc.PREC_FP64), ("mixed", ghc.PREC_MIXED)):
+        # exact scenes, so the scene's unknowns are a solution (known-answer check at 1e-6); with
+        # 0.5 px noise this minimal problem moves its solutions by ~5 % (ill-conditioned)
         b = Batch(torch, "generalized_3views_4pts", H, 77 + args.seed, precision=prec, polish=3, step=step,
-                  start=q, sols=Sq)
+                  start=q, sols=Sq, scene={"noise_px": 0.0})
         if args.tune:
             b.tune()
         g = _capture(torch, b.launch)
@@ -260,10 +262,10 @@ def config_g3v4_mono(args, torch):
             d = np.abs(m - e).max(axis=1) / max(1.0, np.abs(e).max())
             found += bool(d.size and d.min() <= 1e-8)
         E = e64[h][c64[h]]
-        gt_hits += bool(E.size and (np.abs(E - truth[h]).max(axis=1) / np.abs(truth[h]).max()).min() < 1e-2)
+        gt_hits += bool(E.size and (np.abs(E - truth[h]).max(axis=1) / np.abs(truth[h]).max()).min() < 1e-6)
     _line("hypothesis-solves/s at real-sol recall, mixed vs plain FP64 (own start system)", out["mixed"]["value"],
           args, {"workload": "generalized_3views_4pts: start params ~ complex N(0,1) (seed %d), %d start solutions "
-                             "from the monodromy solver, %d seeded scenes (0.5 px noise) per step, path-jump-free "
+                             "from the monodromy solver, %d seeded exact scenes per step, path-jump-free "
                              "step control, FP64 polish" % (args.seed, len(Sq), H)},
           modes=out, recall_mixed_vs_fp64=found / max(1, real), real_solutions_fp64=real,
           ground_truth_found_frac=gt_hits / H, monodromy={"solutions": len(S), "seconds": mono_s})

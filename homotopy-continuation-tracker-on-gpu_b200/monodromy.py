@@ -58,11 +58,11 @@ def _merge(S, cand, tol=MERGE_TOL):
 
 
 def monodromy_solve(pb, x0, p0, target=None, max_loops=200, stall_loops=8, seed=0, log=None):
-    """All (discoverable) solutions of F(x; p0) from one seed solution x0."""
+    """All (discoverable) solutions of F(x; p0) from a seed solution x0 [N] (or a known set [n, N])."""
     if pb.kind != ghc.KIND_P2C:
         raise ValueError("monodromy needs a P2C problem (device coefficient tables)")
     rng = np.random.default_rng(seed)
-    S = np.array([x0], dtype=np.complex128)
+    S = np.atleast_2d(np.asarray(x0, dtype=np.complex128))
     stall = 0
     for loop in range(max_loops):
         if target is not None and len(S) >= target:
@@ -86,7 +86,8 @@ def start_system(pb, seed=0, target=None, log=None):
     """Start parameters q ~ complex N(0,1) (seeded) and all solutions there.
 
     A complexified seed pair is solved by monodromy and the solution set is
-    then moved to q by one parameter-homotopy leg.
+    then moved to q by one parameter-homotopy leg; solutions lost on that leg
+    are recovered by monodromy loops at q from the moved set.
     """
     import scenes
     x0, p_seed = scenes.seed_pair(pb.name, seed=seed)
@@ -94,4 +95,6 @@ def start_system(pb, seed=0, target=None, log=None):
     rng = np.random.default_rng(10_000 + seed)
     q = np.append(rng.normal(size=pb.P) + 1j * rng.normal(size=pb.P), 1.0)
     Sq = _merge(np.zeros((0, pb.N), dtype=complex), track_leg(pb, S, p_seed, q, polish_iters=3))
+    if 0 < len(Sq) < len(S):
+        Sq = monodromy_solve(pb, Sq, q, target=len(S), stall_loops=4, seed=seed + 1, log=log)
     return q, Sq, S

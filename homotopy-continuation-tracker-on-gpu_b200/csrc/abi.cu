@@ -78,6 +78,7 @@ TrackParams base_params(const Problem& pb) {
   p.ht_off = pb.dev.ht_off;
   p.flat_eval = flat_eval_pays(pb.hx_off.data(), pb.N);
   p.scr_slots = row_nonzeros_max(pb.hx_off.data(), pb.N);
+  p.shape = eval_shape_of(pb.kind, pb.Px, pb.Pt);
   // the reference's step control (kernel_HC_Solver_P3P.cu:214): no contraction test, no step cap
   p.corr_tol2 = 1e-6;
   p.first_tol2 = HUGE_VAL;
@@ -97,6 +98,7 @@ PolishParams polish_params(const TrackParams& t, double* endpoints, const uint8_
   q.n_ht_terms = t.n_ht_terms;
   q.flat_eval = t.flat_eval;
   q.scr_slots = t.scr_slots;
+  q.shape = t.shape;
   q.hx_terms = t.hx_terms;
   q.hx_off = t.hx_off;
   q.ht_terms = t.ht_terms;

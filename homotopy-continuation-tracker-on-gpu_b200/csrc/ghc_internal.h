@@ -29,7 +29,7 @@ constexpr int kMaxVarsPerTerm = 7;
 
 // term word layout
 //   bits  0.. 7  integer scale (int8)
-//   bits  8..10  number of variable factors nv (slot N, the constant 1, dropped)
+//   bits  8..10  number of variable slots nv (the same for every term of a table; slot N = the constant 1)
 //   bits 11..20  P2C: coefficient index k (0..1023)
 //   bits 11..16  PH : parameter index a ; bits 17..22 PH: parameter index b
 //   bits 24..58  variable indices, 5 bits each, table order
@@ -77,6 +77,18 @@ inline int flat_eval_pays(const uint16_t* hx_off, int N) {
   return 4 * per_entry > 5 * longest ? 1 : 0;
 }
 
+// Term shape of a problem: (variable slots per H_x term, per H_t term).  Every term of a
+// table has parts - 1 - (coefficient slots) variable slots (compile_tables keeps slot N,
+// the constant 1); the two shapes of the shipped problems get kernels with straight-line
+// term evaluation, any other shape the general kernel.
+enum EvalShape : int { EVAL_GENERAL = 0, EVAL_1_2 = 1, EVAL_2_3 = 2 };
+inline int eval_shape_of(int kind, int Px, int Pt) {
+  const int c = kind == KIND_PH ? 2 : 1, a = Px - 1 - c, b = Pt - 1 - c;
+  return (a == 1 && b == 2) ? EVAL_1_2 : (a == 2 && b == 3) ? EVAL_2_3 : EVAL_GENERAL;
+}
+GHC_HD constexpr int shape_nvx(int S) { return S == EVAL_1_2 ? 1 : S == EVAL_2_3 ? 2 : -1; }
+GHC_HD constexpr int shape_nvt(int S) { return S == EVAL_1_2 ? 2 : S == EVAL_2_3 ? 3 : -1; }
+
 // Everything the tracker kernel needs, by value.
 struct TrackParams {
   // problem
@@ -84,6 +96,7 @@ struct TrackParams {
   int max_steps, max_corr, incr;
   int n_hx_terms, n_ht_terms;
   int flat_eval;              // walk H_x rows (flat_eval_pays() of the tables, or the autotuner's choice)
+  int shape;                  // eval_shape_of() of the problem
   int scr_slots;              // row_nonzeros_max() of the tables
   int variant;                // compiled register-budget variant (0 or 1)
   int variant_f32, flat_eval_f32;  // the FP32 phase's choices in mixed precision
@@ -139,7 +152,7 @@ struct TrackParams {
 struct PolishParams {
   int kind, N, P, M, K;
   int n_hx_terms, n_ht_terms;
-  int flat_eval, scr_slots;
+  int flat_eval, scr_slots, shape;
   const uint64_t* hx_terms;
   const uint16_t* hx_off;
   const uint64_t* ht_terms;

@@ -136,6 +136,7 @@ extern "C" int ghc_track_noalloc(const ghc_problem* h, const ghc_track_args* a, 
   p.ht_off = reinterpret_cast<const uint16_t*>(s + o_hto);
   apply_tuning(pb, a->precision, p);
   p.scr_slots = row_nonzeros_max(pb.hx_off.data(), pb.N);
+  p.shape = eval_shape_of(pb.kind, pb.Px, pb.Pt);
   p.n_items = a->n_hyp * (long long)(a->paths > 0 ? a->paths : pb.paths);
   p.paths_per_hyp = a->paths > 0 ? a->paths : pb.paths;
   p.start_sols = a->d_start_sols;
@@ -210,6 +211,7 @@ extern "C" int ghc_track_noalloc(const ghc_problem* h, const ghc_track_args* a, 
     q.n_ht_terms = p.n_ht_terms;
     q.flat_eval = p.flat_eval;
     q.scr_slots = p.scr_slots;
+    q.shape = p.shape;
     q.hx_terms = p.hx_terms;
     q.hx_off = p.hx_off;
     q.ht_terms = p.ht_terms;

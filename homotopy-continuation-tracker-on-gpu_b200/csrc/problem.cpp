@@ -154,14 +154,15 @@ int compile_tables(const std::vector<int32_t>& hx, const std::vector<int32_t>& h
       }
       w |= (uint64_t)e[1] << 11;
     }
+    // every variable slot of the reference's term, slot N (the constant 1) included, so
+    // that all terms of one table have the same number of factors
     int nv = 0;
     for (int q = 1 + n_coef_slots; q < parts; ++q) {
       const int v = e[q];
-      if (v < 0 || v > N) {
+      if (v < 0 || v > N || v > 31) {
         set_error("variable index out of range in a table");
         return GHC_ERR_RANGE;
       }
-      if (v == N) continue;  // the constant 1
       w |= (uint64_t)v << (24 + 5 * nv);
       ++nv;
     }

@@ -114,13 +114,24 @@ struct Tables {
   const uint16_t* ht_off;
 };
 
-// acc += p * x[v0] * x[v1] ...  (reference monomial term, slot N dropped)
-template <typename R>
+// acc += p * x[v0] * x[v1] ... over the term's variable slots (reference monomial term,
+// dev-eval-indxing-P3P.cuh:70-118; slot N is the constant 1).  Every term of a table has
+// the same number of slots: NV >= 0 fixes it at compile time (straight-line code), NV < 0
+// reads it from the word.
+template <typename R, int NV>
 __device__ __forceinline__ cx<R> acc_term(cx<R> acc, cx<R> p, uint64_t w, const cx<R>* xs) {
-  const int nv = term_nv(w);
-  if (nv == 0) return c_add(acc, p);
-  for (int q = 0; q < nv - 1; ++q) p = c_mul(p, xs[term_var(w, q)]);
-  return c_fma(p, xs[term_var(w, nv - 1)], acc);
+  if constexpr (NV >= 0) {
+    if (NV == 0) return c_add(acc, p);
+#pragma unroll
+    for (int q = 0; q < NV - 1; ++q) p = c_mul(p, xs[term_var(w, q)]);
+    return c_fma(p, xs[term_var(w, NV - 1)], acc);
+  } else {
+    const int nv = term_nv(w);
+    if (nv == 0) return c_add(acc, p);
+#pragma unroll 1
+    for (int q = 0; q < nv - 1; ++q) p = c_mul(p, xs[term_var(w, q)]);
+    return c_fma(p, xs[term_var(w, nv - 1)], acc);
+  }
 }
 
 // c_k(t), c'_k(t) for k = l, l+W, ... (reference eval_parameter_homotopy)
@@ -184,7 +195,7 @@ __device__ __forceinline__ cx<R> term_coef_value(uint64_t w, const cx<R>* ca) {
 template <int N>
 constexpr bool kFlatAlways = N > 16;
 
-template <typename R, int N, int W, int KIND>
+template <typename R, int N, int W, int KIND, int NVX, int NVT>
 __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, const cx<R>* cb, const cx<R>* xs, int r,
                                          bool live, cx<R> (&A)[N], cx<R>& b, int which, bool flat,
                                          unsigned char* scr, unsigned nz) {
@@ -197,7 +208,7 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
         const int base = tb.hx_off[r * N], j0 = tb.hx_off[r * N + i], j1 = tb.hx_off[r * N + i + 1];
         for (int j = j0; j < j1; ++j) {
           const uint64_t w = tb.hx_terms[(j - base) * N + r];
-          acc = acc_term(acc, term_coef_value<R, KIND>(w, ca), w, xs);
+          acc = acc_term<R, NVX>(acc, term_coef_value<R, KIND>(w, ca), w, xs);
         }
       }
       A[i] = acc;
@@ -216,7 +227,7 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
           acc = mk(R(0), R(0));
           cur = i;
         }
-        acc = acc_term(acc, term_coef_value<R, KIND>(w, ca), w, xs);
+        acc = acc_term<R, NVX>(acc, term_coef_value<R, KIND>(w, ca), w, xs);
       }
       if (cur >= 0) *slot(k) = acc;
     }
@@ -240,7 +251,7 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
         p = c_scale((R)term_scale(w), ca[term_pa(w)]);
         p = c_mul(p, ca[term_pb(w)]);
       }
-      h = acc_term(h, p, w, xs);
+      h = acc_term<R, NVT>(h, p, w, xs);
     }
   }
   b = which ? mk(-h.re, -h.im) : h;
@@ -450,13 +461,20 @@ __device__ __forceinline__ unsigned row_mask(const uint16_t* hx_off, int r) {
   return m;
 }
 
+// row l of H_x and the right-hand side, term walk of table shape S (EvalShape)
+template <typename R, int N, int W, int KIND, int S>
+__device__ __forceinline__ void eval_any(const Tables& tb, const SubMem& sm, int l, cx<R> (&A)[N], cx<R>& b,
+                                         int which) {
+  eval_row<R, N, W, KIND, shape_nvx(S), shape_nvt(S)>(tb, view<R>(sm.coefA), view<R>(sm.coefB), view<R>(sm.xs), l,
+                                                      l < N, A, b, which, sm.scr != nullptr, sm.scr, sm.nz);
+}
+
 // one evaluation + solve in precision R; returns this lane's solution component
-template <typename R, int N, int W, int KIND>
+template <typename R, int N, int W, int KIND, int S>
 __device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, int l, int which) {
   cx<R> A[N];
   cx<R> b;
-  eval_row<R, N, W, KIND>(tb, view<R>(sm.coefA), view<R>(sm.coefB), view<R>(sm.xs), l, l < N, A, b, which,
-                          sm.scr != nullptr, sm.scr, sm.nz);
+  eval_any<R, N, W, KIND, S>(tb, sm, l, A, b, which);
   lu_solve<R, N, W>(A, b, l, view<R>(sm.sx), view<R>(sm.sol));
   const cx<R> k = (l < N) ? view<R>(sm.sol)[l] : mk(R(0), R(0));
   return k;
@@ -573,7 +591,7 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 #else
 #define GHC_MINB(N, R, V) track_min_blocks<N, R, V>()
 #endif
-template <typename R, int N, int W, int KIND, int V>
+template <typename R, int N, int W, int KIND, int V, int S>
 __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const TrackParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Tables tb = stage_tables(smem, p.hx_terms, p.hx_off, p.ht_terms, p.ht_off, N, p.n_hx_terms, p.n_ht_terms);
@@ -674,7 +692,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
     // ---------------- one evaluate-and-solve per sub-warp (predictor: -H_t, corrector: H)
     write_track<R, N>(sm, l, x);
     __syncwarp(kFull);
-    const cx<R> v = eval_solve<R, N, W, KIND>(tb, sm, l, rk ? 1 : 0);
+    const cx<R> v = eval_solve<R, N, W, KIND, S>(tb, sm, l, rk ? 1 : 0);
     // ---------------- corrector norms (kernel_HC_Solver_P3P.cu:204-219), all lanes take part
     R ns0 = 0, nc0 = 0;
     if (__any_sync(kFull, corr)) {
@@ -783,7 +801,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
 // -------------------------------------------------------------------------------------------------
 // Newton polish at t = 1 and the residual |H(x,1)| (double); one sub-warp per item
 // -------------------------------------------------------------------------------------------------
-template <int N, int W, int KIND>
+template <int N, int W, int KIND, int S>
 __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Tables tb = stage_tables(smem, p.hx_terms, p.hx_off, p.ht_terms, p.ht_off, N, p.n_hx_terms, p.n_ht_terms);
@@ -819,7 +837,7 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
     for (int it = 0; it < p.iters; ++it) {
       write_track<double, N>(sm, l, x);
       __syncwarp(kFull);
-      const cx<double> d = eval_solve<double, N, W, KIND>(tb, sm, l, 0);
+      const cx<double> d = eval_solve<double, N, W, KIND, S>(tb, sm, l, 0);
       if (conv) x = c_sub(x, d);
     }
     // residual |H(x,1)|
@@ -827,8 +845,7 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
     __syncwarp(kFull);
     cx<double> A[N];
     cx<double> h;
-    eval_row<double, N, W, KIND>(tb, view<double>(sm.coefA), view<double>(sm.coefB), view<double>(sm.xs), l, l < N, A,
-                                 h, 0, flat, sm.scr, sm.nz);
+    eval_any<double, N, W, KIND, S>(tb, sm, l, A, h, 0);
     const double s = tree_sum<double, N, W>(l < N ? c_abs2(h) : 0.0);
     const double s0 = __shfl_sync(kFull, s, leader);
     if (valid) {

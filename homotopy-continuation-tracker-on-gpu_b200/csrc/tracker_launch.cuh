@@ -10,10 +10,10 @@ namespace launch_detail {
 
 constexpr int kBlock = 128;
 
-template <typename R, int N, int KIND, int V>
-int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
+template <typename R, int N, int KIND, int V, int S>
+int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
   constexpr int W = (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
-  auto kern = dev::track_kernel<R, N, W, KIND, V>;
+  auto kern = dev::track_kernel<R, N, W, KIND, V, S>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
   const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
@@ -36,10 +36,22 @@ int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
   return e == cudaSuccess ? 0 : -23;
 }
 
-template <int N, int KIND>
-int launch_polish_t(const PolishParams& p, cudaStream_t s) {
+template <typename R, int N, int KIND, int V>
+int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
+  switch (p.shape) {
+    case EVAL_1_2:
+      return launch_track_s<R, N, KIND, V, EVAL_1_2>(p, s, n_sm);
+    case EVAL_2_3:
+      return launch_track_s<R, N, KIND, V, EVAL_2_3>(p, s, n_sm);
+    default:
+      return launch_track_s<R, N, KIND, V, EVAL_GENERAL>(p, s, n_sm);
+  }
+}
+
+template <int N, int KIND, int S>
+int launch_polish_s(const PolishParams& p, cudaStream_t s) {
   constexpr int W = (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
-  auto kern = dev::polish_kernel<N, W, KIND>;
+  auto kern = dev::polish_kernel<N, W, KIND, S>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
   const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
@@ -50,6 +62,18 @@ int launch_polish_t(const PolishParams& p, cudaStream_t s) {
   if (grid < 1) grid = 1;
   kern<<<(unsigned)grid, kBlock, smem, s>>>(p);
   return cudaGetLastError() == cudaSuccess ? 0 : -23;
+}
+
+template <int N, int KIND>
+int launch_polish_t(const PolishParams& p, cudaStream_t s) {
+  switch (p.shape) {
+    case EVAL_1_2:
+      return launch_polish_s<N, KIND, EVAL_1_2>(p, s);
+    case EVAL_2_3:
+      return launch_polish_s<N, KIND, EVAL_2_3>(p, s);
+    default:
+      return launch_polish_s<N, KIND, EVAL_GENERAL>(p, s);
+  }
 }
 
 }  // namespace launch_detail

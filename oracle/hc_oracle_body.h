@@ -29,8 +29,8 @@
  *     __syncwarp between eval_parameter_homotopy and eval_Jacobian_Hx);
  *   - PH target parameters beyond index N are read per hypothesis (the
  *     reference reads them without the hypothesis offset);
- *   - padding terms (integer scale 0) are skipped and variable slot N (the
- *     constant 1) is not multiplied in;
+ *   - padding terms (integer scale 0) are skipped (variable slot N, the
+ *     constant 1, is multiplied in like any other slot, as in the reference);
  *   - the pivot reciprocal is conj(b)/|b|^2 (one reciprocal); the back
  *     substitution multiplies by the reciprocal formed during elimination;
  *   - pivot magnitudes are compared after quantisation to their upper bits
@@ -82,15 +82,13 @@ static REAL SFX(tree_sum)(const REAL* v, int n) {
   return buf[0];
 }
 
-/* accumulate one monomial term: acc += s * first * x[v0] * x[v1] ... (slot N dropped) */
-static inline CX SFX(acc_term)(CX acc, CX p, const int32_t* vars, int nvar_raw, const CX* x, int N) {
-  int vs[8];
-  int nv = 0;
-  for (int q = 0; q < nvar_raw; ++q)
-    if (vars[q] != N) vs[nv++] = vars[q];
-  if (nv == 0) return SFX(c_add)(acc, p);
-  for (int q = 0; q < nv - 1; ++q) p = SFX(c_mul)(p, x[vs[q]]);
-  return SFX(c_fma)(p, x[vs[nv - 1]], acc);
+/* accumulate one monomial term: acc += s * first * x[v0] * x[v1] ... over every variable
+ * slot of the table, slot N being the constant 1 (GPU-HC/magmaHC/gpu-idx-evals/
+ * dev-eval-indxing-P3P.cuh:70-118); the last product is fused into the accumulation */
+static inline CX SFX(acc_term)(CX acc, CX p, const int32_t* vars, int nvar, const CX* x) {
+  if (nvar == 0) return SFX(c_add)(acc, p);
+  for (int q = 0; q < nvar - 1; ++q) p = SFX(c_mul)(p, x[vars[q]]);
+  return SFX(c_fma)(p, x[vars[nvar - 1]], acc);
 }
 
 typedef struct {
@@ -157,13 +155,13 @@ static void SFX(eval_hx_row)(const orc_problem* pb, const COEFS* cf, const CX* x
         for (int q = 0; q < Px; ++q) tm[q] = e[q];
         if (tm[0] == 0) continue;
         CX p = SFX(c_scale)((REAL)tm[0], cf->c[tm[1]]);
-        acc = SFX(acc_term)(acc, p, tm + 2, Px - 2, x, N);
+        acc = SFX(acc_term)(acc, p, tm + 2, Px - 2, x);
       } else {
         for (int q = 0; q < Px; ++q) tm[q] = pb->hx_idx[((size_t)i * Tx * Px + (size_t)j * Px + q) * N + r];
         if (tm[0] == 0) continue;
         CX p = SFX(c_scale)((REAL)tm[0], cf->ph[tm[1]]);
         p = SFX(c_mul)(p, cf->ph[tm[2]]);
-        acc = SFX(acc_term)(acc, p, tm + 3, Px - 3, x, N);
+        acc = SFX(acc_term)(acc, p, tm + 3, Px - 3, x);
       }
     }
     A[i] = acc;
@@ -181,7 +179,7 @@ static CX SFX(eval_h_row)(const orc_problem* pb, const COEFS* cf, const CX* x, i
       for (int q = 0; q < Pt; ++q) tm[q] = e[q];
       if (tm[0] == 0) continue;
       CX p = SFX(c_scale)((REAL)tm[0], which ? cf->cp[tm[1]] : cf->c[tm[1]]);
-      acc = SFX(acc_term)(acc, p, tm + 2, Pt - 2, x, N);
+      acc = SFX(acc_term)(acc, p, tm + 2, Pt - 2, x);
     } else {
       for (int q = 0; q < Pt; ++q) tm[q] = pb->ht_idx[((size_t)j * Pt + q) * N + r];
       if (tm[0] == 0) continue;
@@ -193,7 +191,7 @@ static CX SFX(eval_h_row)(const orc_problem* pb, const COEFS* cf, const CX* x, i
         p = SFX(c_scale)((REAL)tm[0], cf->ph[tm[1]]);
         p = SFX(c_mul)(p, cf->ph[tm[2]]);
       }
-      acc = SFX(acc_term)(acc, p, tm + 3, Pt - 3, x, N);
+      acc = SFX(acc_term)(acc, p, tm + 3, Pt - 3, x);
     }
   }
   return acc;

@@ -205,9 +205,10 @@ def real_targets(ob, n_hyp, seed):
                                   "uncalibrated_trifocal_rel_pos_CY"])
 def test_mixed_precision_recall(name):
     """FP32 tracking to t = 0.9 then FP64, both runs with path-jump-free step control:
-    >= 99.5% of the FP64 run's real endpoints are found by the mixed run within 1e-8."""
+    >= 99.5% of the FP64 run's real endpoints are found by the mixed run within 1e-8
+    (8 hypotheses: several hundred real endpoints, so that the bar admits a miss)."""
     pb, ob = ghc.Problem(name), O.Problem(name)
-    tg = real_targets(ob, 2, 9)
+    tg = real_targets(ob, 8, 9)
     w64, _ = run_gpu(pb, ob, tg, ghc.PREC_FP64, polish=3, **ROBUST)
     wmx, _ = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=3, t_switch=0.9, **ROBUST)
     e64, emx = to_cx(w64.endpoints), to_cx(wmx.endpoints)

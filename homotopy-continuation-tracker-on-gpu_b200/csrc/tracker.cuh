@@ -448,8 +448,10 @@ struct SubMem {
   unsigned char* sol;    // solution [N]
   unsigned char* state;  // per lane: RK base point x0 [W], RK accumulator [W]
   unsigned char* scr;    // H_x row scratch [slots][W], null unless the evaluation is flat
+  unsigned char* rec;    // the path's scalar state while the sub-warp evaluates and solves [kRecBytes]
   unsigned nz;           // this lane's row: bit i set when H_x entry (row, i) has terms
 };
+constexpr int kRecBytes = 128;
 
 // bit i set when row r of H_x has terms in column i (0 for lanes beyond the rows)
 template <int N>
@@ -503,15 +505,18 @@ __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t
 __host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
   return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(N * N + 1 + N + 1));
 }
-// per sub-warp, in complex values of esz bytes: coefficient buffers [2 Mc], track [N+1],
-// two pivot rows [2 (N+1)], solution [N], lane state [2 W], scratch slots [slots W] (flat)
+// per sub-warp: the path record [kRecBytes], then in complex values of esz bytes: coefficient
+// buffers [2 Mc], track [N+1], two pivot rows [2 (N+1)], solution [N], lane state [2 W], scratch
+// slots [slots W] (flat)
 __host__ __device__ inline size_t sub_bytes(int N, int Mc, int W, int slots, int esz) {
-  return align16((size_t)esz * (2 * (size_t)Mc + 3 * (N + 1) + N + 2 * W + (size_t)slots * W));
+  return align16((size_t)esz * (2 * (size_t)Mc + 3 * (N + 1) + N + 2 * W + (size_t)slots * W)) + kRecBytes;
 }
 template <typename R>
 __device__ __forceinline__ SubMem sub_layout(unsigned char* base, int N, int Mc, int W, bool flat) {
   constexpr int e = sizeof(cx<R>);
   SubMem sm;
+  sm.rec = base;
+  base += kRecBytes;
   sm.coefA = base;
   sm.coefB = base + e * (size_t)Mc;
   sm.xs = base + 2 * e * (size_t)Mc;
@@ -678,6 +683,55 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
   };
   if (alive) init_path(item);
 
+  // The path's scalar state (the same in every lane of the sub-warp) and this lane's track
+  // component wait in shared memory while the sub-warp evaluates and solves, so that no
+  // register holds them across the LU (register relief).  Volatile: stored and reloaded,
+  // never forwarded.
+  volatile R* rec_r = reinterpret_cast<volatile R*>(sm.rec);
+  volatile long long* rec_l = reinterpret_cast<volatile long long*>(sm.rec + 6 * sizeof(R));
+  volatile int* rec_i = reinterpret_cast<volatile int*>(sm.rec + 6 * sizeof(R) + 2 * sizeof(long long));
+  auto stash = [&]() {
+    rec_r[0] = t0;
+    rec_r[1] = dt;
+    rec_r[2] = t_step;
+    rec_r[3] = half;
+    rec_r[4] = dt_pre;
+    rec_r[5] = coef_t;
+    rec_l[0] = item;
+    rec_l[1] = hyp;
+    rec_i[0] = step;
+    rec_i[1] = ncorr;
+    rec_i[2] = phase;
+    rec_i[3] = cit;
+    rec_i[4] = nfail;
+    rec_i[5] = nsucc;
+    rec_i[6] = (alive ? 1 : 0) | (finished ? 2 : 0) | (end_zone ? 4 : 0) | (success ? 8 : 0) | (inf ? 16 : 0);
+  };
+  auto unstash = [&]() {
+    t0 = rec_r[0];
+    dt = rec_r[1];
+    t_step = rec_r[2];
+    half = rec_r[3];
+    dt_pre = rec_r[4];
+    coef_t = rec_r[5];
+    item = rec_l[0];
+    hyp = rec_l[1];
+    step = rec_i[0];
+    ncorr = rec_i[1];
+    phase = rec_i[2];
+    cit = rec_i[3];
+    nfail = rec_i[4];
+    nsucc = rec_i[5];
+    const int f = rec_i[6];
+    alive = f & 1;
+    finished = (f >> 1) & 1;
+    end_zone = (f >> 2) & 1;
+    success = (f >> 3) & 1;
+    inf = (f >> 4) & 1;
+    const volatile cx<R>* xv = reinterpret_cast<const volatile cx<R>*>(sm.xs);
+    x = (l < N) ? mk(xv[l].re, xv[l].im) : mk(R(0), R(0));
+  };
+
   while (__any_sync(kFull, alive)) {
     const bool served = alive && !finished;
     const bool rk = served && phase < 4;
@@ -691,8 +745,10 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
     }
     // ---------------- one evaluate-and-solve per sub-warp (predictor: -H_t, corrector: H)
     write_track<R, N>(sm, l, x);
+    stash();
     __syncwarp(kFull);
     const cx<R> v = eval_solve<R, N, W, KIND, S>(tb, sm, l, rk ? 1 : 0);
+    unstash();
     // ---------------- corrector norms (kernel_HC_Solver_P3P.cu:204-219), all lanes take part
     R ns0 = 0, nc0 = 0;
     if (__any_sync(kFull, corr)) {

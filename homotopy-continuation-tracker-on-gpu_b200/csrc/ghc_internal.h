@@ -32,6 +32,7 @@ constexpr int kMaxVarsPerTerm = 7;
 //   bits  8..10  number of variable slots nv (the same for every term of a table; slot N = the constant 1)
 //   bits 11..20  P2C: coefficient index k (0..1023)
 //   bits 11..16  PH : parameter index a ; bits 17..22 PH: parameter index b
+//   bit  23      H_x terms: the last term of its entry (row, column)
 //   bits 24..58  variable indices, 5 bits each, table order
 //   bits 59..63  H_x terms: the Jacobian column of the term (its row is implied by the CSR row)
 GHC_HD inline int term_scale(uint64_t w) { return (int)(int8_t)(w & 0xffu); }
@@ -41,6 +42,8 @@ GHC_HD inline int term_pa(uint64_t w) { return (int)((w >> 11) & 0x3fu); }
 GHC_HD inline int term_pb(uint64_t w) { return (int)((w >> 17) & 0x3fu); }
 GHC_HD inline int term_var(uint64_t w, int q) { return (int)((w >> (24 + 5 * q)) & 31u); }
 GHC_HD inline int term_col(uint64_t w) { return (int)(w >> 59); }
+constexpr uint64_t kTermLast = 1ull << 23;
+GHC_HD inline bool term_last(uint64_t w) { return (w & kTermLast) != 0; }
 
 // Whether the tracker should walk each H_x row as one term list (staging the
 // entries in shared memory) rather than entry by entry.  Entry by entry, a

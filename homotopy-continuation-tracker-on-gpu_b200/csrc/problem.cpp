@@ -185,6 +185,8 @@ int compile_tables(const std::vector<int32_t>& hx, const std::vector<int32_t>& h
         if (rc) return rc;
         hx_terms.push_back(w | (uint64_t)i << 59);
       }
+      // the entry's last term ends its sum in the row-wise walk
+      if (hx_terms.size() > hx_off[(size_t)r * N + i]) hx_terms.back() |= kTermLast;
     }
   }
   hx_off[(size_t)N * N] = (uint16_t)hx_terms.size();

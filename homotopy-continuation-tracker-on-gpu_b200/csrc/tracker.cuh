@@ -183,7 +183,7 @@ __device__ __forceinline__ cx<R> term_coef_value(uint64_t w, const cx<R>* ca) {
 // Row r of H_x into A, and b = H (which = 0) or -H_t (which = 1).
 //
 // Flat (always above 16 unknowns, else when the problem's flat_eval is set):
-// the row's terms are walked as one list (CSR row r, column in the term word),
+// the row's terms are walked as one list (CSR row r, entry ends flagged in the term word),
 // so a sub-warp spends max_r(terms of row r) iterations instead of
 // sum_i max_r(terms of entry (r, i)).  The k-th non-zero entry of the row is
 // staged in the sub-warp's scratch slot scr[k][r] (only as many slots as the
@@ -216,20 +216,16 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
   } else {
     if (live) {
       const int len = tb.hx_off[r * N + N] - tb.hx_off[r * N];
-      int cur = -1, k = -1;
+      int k = 0;
       cx<R> acc = mk(R(0), R(0));
       for (int q = 0; q < len; ++q) {
         const uint64_t w = tb.hx_terms[q * N + r];
-        const int i = term_col(w);
-        if (i != cur) {
-          if (cur >= 0) *slot(k) = acc;
-          ++k;
-          acc = mk(R(0), R(0));
-          cur = i;
-        }
         acc = acc_term<R, NVX>(acc, term_coef_value<R, KIND>(w, ca), w, xs);
+        if (term_last(w)) {  // the entry's sum is complete
+          *slot(k++) = acc;
+          acc = mk(R(0), R(0));
+        }
       }
-      if (cur >= 0) *slot(k) = acc;
     }
 #pragma unroll
     for (int i = 0; i < N; ++i)
@@ -315,7 +311,6 @@ template <typename R, int N, int W>
 __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
   const bool live = l < N;
   int pos = l;
-  cx<R> myrcp = mk(R(0), R(0));
   static_for<0, N>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     cx<R>* px = sx + (i & 1) * (N + 1);
@@ -332,8 +327,11 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
     __syncwarp(kFull);
     const cx<R> p_i = px[i];
     const bool zero = (fabs(p_i.re) + fabs(p_i.im) == R(0));
-    const cx<R> rc = c_rcp(zero ? mk(R(0), R(0)) : p_i);
-    if (is_piv) myrcp = rc;
+    // (a zero pivot's reciprocal is NaN, as the oracle's c_rcp(0))
+    const cx<R> rc = c_rcp(p_i);
+    // the pivot row's reciprocal waits in the solution slot of its position until the back
+    // substitution (the slot is written there only after this lane has read it)
+    if (is_piv) sol[i] = rc;
     // rows below the pivot take the update, the others keep their values
     const bool upd = live && pos > i && !zero;
 #if GHC_LU_SELECT
@@ -360,7 +358,7 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
   });
   static_for<0, N>([&](auto ic) {
     constexpr int i = N - 1 - decltype(ic)::value;
-    if (live && pos == i) sol[i] = c_mul(b, myrcp);
+    if (live && pos == i) sol[i] = c_mul(b, sol[i]);
     __syncwarp(kFull);
     const cx<R> xi = sol[i];
     if (live && pos < i) b = c_fnma(A[i], xi, b);

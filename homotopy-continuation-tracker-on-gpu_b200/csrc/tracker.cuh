@@ -540,17 +540,17 @@ __device__ __forceinline__ cx<R> load_cx(const void* base, bool f64, long long i
 // complex values) dominates the registers, so small systems afford more.  Two
 // compiled variants per size and precision; the autotuner (ghc_autotune) picks
 // one per problem.  Variant 0 is the best of B200 sweeps over the shipped
-// problems (FP64 N = 3 at 6 -- at 8 the 64 registers spill --, N = 6 and
-// N = 12 at 4); variant 1 trades registers for more CTAs per SM (N = 12:
-// better for the uncalibrated trifocal problem, worse for the generalized
-// 3-view problem, which have the same size; N = 30: FP64 342 vs 308 hyp/s at
-// 3 instead of 2 CTAs, FP32 488 vs 450 at 5 instead of 3).
+// problems (512 hypotheses, autotuning off, 3..7 CTAs): FP64 N = 3 at 6 (at 8
+// the 64 registers spill), N = 6 flat within noise, N = 12 at 5 (generalized
+// 3-view 5360 vs 5326 hyp/s at 4, uncalibrated trifocal 1376 vs 1348; 6 and 7
+// spill), N = 30 at 3 (406 vs 397 at 4); FP32 N = 12 at 7, N = 30 at 5 (577
+// vs 552 at 3).  Variant 1 is the runner-up budget.
 template <int N, typename R, int V>
 constexpr int track_min_blocks() {
-  return V == 0 ? (sizeof(R) == 8 ? (N <= 4 ? 6 : N <= 12 ? 4 : N <= 18 ? 3 : 2)
-                                  : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 3))
-                : (sizeof(R) == 8 ? (N <= 4 ? 8 : N <= 12 ? 5 : N <= 18 ? 4 : 3)
-                                  : (N <= 8 ? 10 : N <= 12 ? 8 : 5));
+  return V == 0 ? (sizeof(R) == 8 ? (N <= 4 ? 6 : N <= 8 ? 4 : N <= 12 ? 5 : 3)
+                                  : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 5))
+                : (sizeof(R) == 8 ? (N <= 4 ? 8 : N <= 8 ? 6 : N <= 12 ? 4 : N <= 18 ? 4 : 2)
+                                  : (N <= 8 ? 10 : N <= 12 ? 8 : N <= 18 ? 5 : 4));
 }
 
 __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64_t* g_hx, const uint16_t* g_hxo,

@@ -76,7 +76,7 @@ def parse():
     ap.add_argument("--step", default="reference", choices=["reference", "robust"], help="for --config problem")
     ap.add_argument("--tune", type=int, default=1, help="autotune the launch before timing (1) or keep the defaults (0)")
     ap.add_argument("--config", default="g3v4", choices=["g3v4", "cy", "p3p_td", "mix", "served", "g3v4_mono",
-                                                          "problem"],
+                                                          "problem", "latency"],
                     help="g3v4: the headline (default); the others are the remaining workloads of the scope")
     return ap.parse_args()
 

@@ -612,14 +612,22 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
   cx<R>& x0 = view<R>(sm.state)[l];
   cx<R>& sols = view<R>(sm.state)[W + l];
 
+  // Paths go to sub-warps in order, or, when the launch has fewer paths than one wave of warps
+  // (spread), one path to each warp: a lone instance then has no two paths in one warp, whose
+  // phases would serialise each other's step logic.  The other sub-warps of the warp track the
+  // same path in lockstep (identical work, so no divergence and no idle lanes computing on stale
+  // shared memory); only the first one (primary) writes results and takes the next path.
   const int subs_per_cta = blockDim.x / W;
-  const long long n_sw = (long long)gridDim.x * subs_per_cta;
+  const int slots_per_cta = p.spread ? (int)(blockDim.x / 32) : subs_per_cta;
+  const long long n_sw = (long long)gridDim.x * slots_per_cta;
+  const bool primary = !p.spread || lane < W;
   const int leader = lane - l;
   const bool handover = p.t_handover > 0.0 || p.fail_limit > 0;
   const R t_hand = (R)p.t_handover;
 
   // per-path state (replicated across the sub-warp's lanes)
-  long long item = (long long)blockIdx.x * subs_per_cta + g;
+  long long item = p.spread ? (long long)blockIdx.x * slots_per_cta + (threadIdx.x >> 5)
+                            : (long long)blockIdx.x * subs_per_cta + g;
   bool alive = item < p.n_items;
   long long hyp = 0;
   cx<R> x = mk(R(0), R(0));
@@ -820,7 +828,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
     }
 
     // ---------------- finished paths: write out and take the next path
-    if (done) {
+    if (done && primary) {
       R* ep = reinterpret_cast<R*>(p.endpoints) + 2 * item * p.ld_out;
       if (l < N) {
         ep[2 * l] = x.re;
@@ -842,8 +850,8 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
       }
     }
     long long nxt = 0;
-    if (done && l == 0) nxt = n_sw + (long long)atomicAdd(p.counter, 1);
-    nxt = __shfl_sync(kFull, nxt, leader);
+    if (done && l == 0 && primary) nxt = n_sw + (long long)atomicAdd(p.counter, 1);
+    nxt = __shfl_sync(kFull, nxt, p.spread ? 0 : leader);
     if (done) {
       item = nxt;
       alive = item < p.n_items;

@@ -24,14 +24,19 @@ int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
   int occ = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlock, smem);
   if (e != cudaSuccess || occ < 1) return -21;
-  // persistent grid: fill the GPU once, but never launch more sub-warps than items
+  // persistent grid: fill the GPU once, but never launch more sub-warps than items; a launch
+  // with fewer paths than one warp per scheduler of every SM gives each path its own warp
+  TrackParams q = p;
+  const int warps = kBlock / 32;
+  q.spread = (W < 32 && p.n_items <= (long long)n_sm * warps) ? 1 : 0;
+  const int per_cta = q.spread ? warps : subs;
   long long grid = (long long)occ * n_sm;
-  const long long need = (p.n_items + subs - 1) / subs;
+  const long long need = (p.n_items + per_cta - 1) / per_cta;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
   e = cudaMemsetAsync(p.counter, 0, sizeof(int), s);
   if (e != cudaSuccess) return -22;
-  kern<<<(unsigned)grid, kBlock, smem, s>>>(p);
+  kern<<<(unsigned)grid, kBlock, smem, s>>>(q);
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : -23;
 }

@@ -14,6 +14,9 @@ g3v4_mono  generalized 3-view with start parameters ~ complex N(0,1) and
          start solutions from the monodromy solver, plain FP64 vs mixed.
 problem  any problem folder (--problem), --hyp hypotheses per launch, one
          precision (--precision) and step control (--step): the tracker alone.
+latency  one instance per launch on each problem's shipped parameters (P3P,
+         5-point, generalized 3-view, CY, 30x30), FP32 / FP64 / mixed, p50/p99
+         ms beside the reference's published single-instance times.
 
 Each prints one JSON line with the bench contract's keys.
 """
@@ -53,10 +56,13 @@ class Batch:
     """One problem's batch: inputs on the device, a workspace, and the launch."""
 
     def __init__(self, torch, name, H, seed, precision=ghc.PREC_FP64, polish=0, step=None, start=None, sols=None,
-                 scene=None):
+                 scene=None, shipped=False):
         self.pb = ghc.Problem(name)
         s, t = self.pb.params()
-        st, tg, truth = scenes.targets_for(name, H, seed, s, t, **(scene or {}))
+        if shipped:  # the problem folder's own instance: its start and target parameters
+            st, tg, truth = s, np.repeat(np.asarray(t)[None, :], H, axis=0), None
+        else:
+            st, tg, truth = scenes.targets_for(name, H, seed, s, t, **(scene or {}))
         if start is not None:
             st = start
         self.name, self.H, self.truth, self.targets = name, H, truth, tg
@@ -299,6 +305,51 @@ def config_problem(args, torch):
           b.pb.kind == ghc.KIND_P2C else 1))
 
 
+# The reference's published single-instance times (ms per problem instance, complex FP32 kernels, GPU
+# model not stated): GPU-HC README.md:41-63.
+PUBLISHED_MS = [("P3P", 0.15), ("5pt_rel_pos_alg_form_quat", 1.77), ("generalized_3views_4pts", 4.77),
+                ("uncalibrated_trifocal_rel_pos_CY", 16.67), ("trifocal_2op1p_30x30", 54.44)]
+
+
+def config_latency(args, torch):
+    """One instance per launch: each problem's shipped start and target parameters, the reference's
+    step control, the tracker timed by CUDA events with the coefficients resident (the reference
+    builds them on the host before its kernel), and device P2C + tracker beside it, in FP32 (the
+    reference's precision), FP64 and mixed; p50 / p99 beside the reference's published time."""
+    n = max(args.steps, 30)
+    out, ratios, launches = {}, [], 0
+    for name, pub in PUBLISHED_MS:
+        row = {"published_ms": pub}
+        for pname, prec in (("fp32", ghc.PREC_FP32), ("fp64", ghc.PREC_FP64), ("mixed", ghc.PREC_MIXED)):
+            b = Batch(torch, name, 1, 0, precision=prec, shipped=True)
+            inp = b._inputs()  # coefficients resident: the tracker alone, as the reference times it
+            lat, lat_p2c = [], []
+            for i in range(args.warmup + n):
+                for fn, acc in ((lambda: ghc.track(b.pb, b.ws, b.d_sols, **inp, **b.kw), lat), (b.launch, lat_p2c)):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    fn()
+                    e1.record()
+                    e1.synchronize()
+                    if i >= args.warmup:
+                        acc.append(e0.elapsed_time(e1))
+            row[pname] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                          "p2c_and_track_p50_ms": float(np.percentile(lat_p2c, 50)),
+                          "converged": int(b.ws.conv.sum()), "paths": b.paths}
+            launches += n * ((2 if prec == ghc.PREC_MIXED else 1) * 2 + (1 if b.pb.kind == ghc.KIND_P2C else 0))
+        row["fp32_speedup_vs_published"] = pub / row["fp32"]["p50_ms"]
+        ratios.append(row["fp32_speedup_vs_published"])
+        out[name] = row
+    gm = float(np.exp(np.mean(np.log(ratios))))
+    _line("single-instance latency vs the reference's published times (geometric mean of ratios, FP32)", gm, args,
+          {"workload": "one instance per launch: the shipped start/target parameters of P3P, 5-point, "
+                       "generalized 3-view, uncalibrated trifocal CY and trifocal 30x30; reference step control; "
+                       "p50 over %d launches each" % n},
+          unit="x (published ms / p50 ms)", data="the problem folders' own instances", problems=out,
+          gpu_launches=launches)
+
+
 def config_served(args, torch):
     import serve
     serve.bench(args, torch)
@@ -308,4 +359,4 @@ def run(args):
     import torch
     torch.cuda.set_device(0)
     {"cy": config_cy, "p3p_td": config_p3p_td, "mix": config_mix, "served": config_served,
-     "g3v4_mono": config_g3v4_mono, "problem": config_problem}[args.config](args, torch)
+     "g3v4_mono": config_g3v4_mono, "problem": config_problem, "latency": config_latency}[args.config](args, torch)

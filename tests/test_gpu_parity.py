@@ -337,3 +337,29 @@ def test_dropin_reference_abi(name, prec):
     c = r["conv"] == 1
     assert np.all(d[c] == 1)
     assert np.allclose(d[~c].real, r["t_end"][~c]) and np.allclose(d[~c].imag, r["dt_end"][~c])
+
+
+@pytest.mark.parametrize("name,precision", [("P3P", ghc.PREC_FP64), ("P3P", ghc.PREC_FP32),
+                                            ("5pt_rel_pos_alg_form_quat", ghc.PREC_MIXED)])
+def test_single_instance_spread_equals_batch(name, precision):
+    """A launch with fewer paths than one warp per scheduler gives each path its own warp (spread);
+    the same instance inside a large batch runs sub-warps side by side: both are bit-identical
+    with each other, and the single one with the oracle."""
+    pb, ob = ghc.Problem(name), O.Problem(name)
+    tg = ob.target_params[None, :]
+    one, oargs = run_gpu(pb, ob, tg, precision)
+    assert pb.paths <= 148 * 4  # spread
+    many, _ = run_gpu(pb, ob, np.repeat(tg, 100, axis=0), precision)
+    assert 100 * pb.paths > 148 * 4  # packed sub-warps
+    n = pb.paths
+    assert np.array_equal(to_cx(one.endpoints), to_cx(many.endpoints)[:n], equal_nan=True)
+    for f in ("conv", "inf", "status", "steps", "corr"):
+        assert np.array_equal(getattr(one, f).cpu().numpy(), getattr(many, f).cpu().numpy()[:n])
+    if precision == ghc.PREC_FP32:
+        oargs = {k: (v.astype(np.complex64) if isinstance(v, np.ndarray) else v) for k, v in oargs.items()}
+        r = O.track(ob, ob.start_sols.astype(np.complex64), precision="f", nthreads=NCPU, **oargs)
+    elif precision == ghc.PREC_MIXED:
+        r = O.track(ob, ob.start_sols, precision="mixed", t_switch=0.9, nthreads=NCPU, **oargs)
+    else:
+        r = O.track(ob, ob.start_sols, nthreads=NCPU, **oargs)
+    compare(one, r)

@@ -141,7 +141,7 @@ struct TrackParams {
   double* t_end;
   double* dt_end;
   // scratch
-  int* counter;            // one int, zero before launch
+  int* counter;            // one int, used as unsigned: zeroed before every launch that steals work
   int spread;              // set by the launcher: one path per warp (launches smaller than one wave)
   // handover (first phase of mixed precision): stop at t_handover (> 0) or after
   // fail_limit (> 0) consecutive failed steps or on divergence, keeping the last accepted point

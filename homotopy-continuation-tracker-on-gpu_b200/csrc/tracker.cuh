@@ -850,7 +850,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
       }
     }
     long long nxt = 0;
-    if (done && l == 0 && primary) nxt = n_sw + (long long)atomicAdd(p.counter, 1);
+    if (done && l == 0 && primary) nxt = n_sw + (long long)atomicAdd(reinterpret_cast<unsigned*>(p.counter), 1u);
     nxt = __shfl_sync(kFull, nxt, p.spread ? 0 : leader);
     if (done) {
       item = nxt;

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "ghc_internal.h"
 #include "tracker.cuh"
 
@@ -19,11 +21,29 @@ int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
   const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
   const size_t smem =
       dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, slots, 2 * (int)sizeof(R));
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // Host calls in the launch path delay small launches, so per instantiation and device the
+  // shared-memory attribute is only ever raised (to the largest size asked for, so a concurrent
+  // launch never sees it below its own size) and the occupancy of the last size is kept.
+  constexpr int kDevs = 16;
+  static std::atomic<long long> attr_max[kDevs], occ_key[kDevs];
+  static std::atomic<int> occ_val[kDevs];
+  int dev_id = 0;
+  cudaError_t e = cudaGetDevice(&dev_id);
   if (e != cudaSuccess) return -20;
-  int occ = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlock, smem);
-  if (e != cudaSuccess || occ < 1) return -21;
+  const int d = dev_id & (kDevs - 1);
+  long long have = attr_max[d].load();
+  while (have < (long long)smem) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return -20;
+    if (attr_max[d].compare_exchange_weak(have, (long long)smem)) break;
+  }
+  int occ = occ_key[d].load() == (long long)smem + 1 ? occ_val[d].load() : 0;
+  if (occ < 1) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlock, smem);
+    if (e != cudaSuccess || occ < 1) return -21;
+    occ_val[d].store(occ);
+    occ_key[d].store((long long)smem + 1);
+  }
   // persistent grid: fill the GPU once, but never launch more sub-warps than items; a launch
   // with fewer paths than one warp per scheduler of every SM gives each path its own warp
   TrackParams q = p;
@@ -34,8 +54,12 @@ int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
   const long long need = (p.n_items + per_cta - 1) / per_cta;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
-  e = cudaMemsetAsync(p.counter, 0, sizeof(int), s);
-  if (e != cudaSuccess) return -22;
+  // spread: every path is placed at launch and the (unsigned) counter only ever yields items
+  // >= n_items, so it needs no reset
+  if (!q.spread) {
+    e = cudaMemsetAsync(p.counter, 0, sizeof(int), s);
+    if (e != cudaSuccess) return -22;
+  }
   kern<<<(unsigned)grid, kBlock, smem, s>>>(q);
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : -23;

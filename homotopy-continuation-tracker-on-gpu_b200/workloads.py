@@ -314,8 +314,9 @@ PUBLISHED_MS = [("P3P", 0.15), ("5pt_rel_pos_alg_form_quat", 1.77), ("generalize
 def config_latency(args, torch):
     """One instance per launch: each problem's shipped start and target parameters, the reference's
     step control, the tracker timed by CUDA events with the coefficients resident (the reference
-    builds them on the host before its kernel), and device P2C + tracker beside it, in FP32 (the
-    reference's precision), FP64 and mixed; p50 / p99 beside the reference's published time."""
+    builds them on the host before its kernel) as replays of a captured launch, and beside it eager
+    launches and eager device P2C + tracker, in FP32 (the reference's precision), FP64 and mixed;
+    p50 / p99 beside the reference's published time."""
     n = max(args.steps, 30)
     out, ratios, launches = {}, [], 0
     for name, pub in PUBLISHED_MS:
@@ -323,9 +324,14 @@ def config_latency(args, torch):
         for pname, prec in (("fp32", ghc.PREC_FP32), ("fp64", ghc.PREC_FP64), ("mixed", ghc.PREC_MIXED)):
             b = Batch(torch, name, 1, 0, precision=prec, shipped=True)
             inp = b._inputs()  # coefficients resident: the tracker alone, as the reference times it
-            lat, lat_p2c = [], []
+            track = lambda: ghc.track(b.pb, b.ws, b.d_sols, **inp, **b.kw)  # noqa: E731
+            # replays of a captured launch (device time, as a C++ caller that captures its solve sees
+            # it), beside eager launches from Python (host launch overhead inside the events) and
+            # eager device P2C + tracker
+            g = _capture(torch, track)
+            lat, lat_eager, lat_p2c = [], [], []
             for i in range(args.warmup + n):
-                for fn, acc in ((lambda: ghc.track(b.pb, b.ws, b.d_sols, **inp, **b.kw), lat), (b.launch, lat_p2c)):
+                for fn, acc in ((g.replay, lat), (track, lat_eager), (b.launch, lat_p2c)):
                     e0 = torch.cuda.Event(enable_timing=True)
                     e1 = torch.cuda.Event(enable_timing=True)
                     e0.record()
@@ -335,9 +341,10 @@ def config_latency(args, torch):
                     if i >= args.warmup:
                         acc.append(e0.elapsed_time(e1))
             row[pname] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                          "eager_p50_ms": float(np.percentile(lat_eager, 50)),
                           "p2c_and_track_p50_ms": float(np.percentile(lat_p2c, 50)),
                           "converged": int(b.ws.conv.sum()), "paths": b.paths}
-            launches += n * ((2 if prec == ghc.PREC_MIXED else 1) * 2 + (1 if b.pb.kind == ghc.KIND_P2C else 0))
+            launches += n * ((2 if prec == ghc.PREC_MIXED else 1) * 3 + (1 if b.pb.kind == ghc.KIND_P2C else 0))
         row["fp32_speedup_vs_published"] = pub / row["fp32"]["p50_ms"]
         ratios.append(row["fp32_speedup_vs_published"])
         out[name] = row

@@ -315,7 +315,7 @@ int ghc_problem_get_info(const ghc_problem* h, ghc_problem_info* info) {
   info->max_steps = pb.max_steps;
   info->max_corr = pb.max_corr;
   info->incr_steps = pb.incr;
-  info->n_hx_terms = (int)pb.hx_off.back();
+  info->n_hx_terms = (int)pb.hx_off[(size_t)pb.N * pb.N];
   info->n_ht_terms = (int)pb.ht_off.back();
   info->has_p2c_terms = pb.has_terms ? 1 : 0;
   info->subwarp = track_subwarp_width(pb.N);
@@ -504,7 +504,7 @@ int ghc_count_results(int32_t N, int32_t paths, const double* z, const uint8_t* 
 }
 
 int ghc_set_tuning(ghc_problem* h, int32_t precision, int32_t variant, int32_t flat) {
-  if (!h || (variant != 0 && variant != 1) || flat < -1 || flat > 1 ||
+  if (!h || (variant != 0 && variant != 1) || flat < -1 || flat > 2 ||
       (precision != GHC_PREC_FP64 && precision != GHC_PREC_FP32 && precision != GHC_PREC_MIXED)) {
     set_error("bad tuning argument");
     return GHC_ERR_ARG;
@@ -548,7 +548,8 @@ int ghc_autotune(ghc_problem* h, const ghc_track_args* a, void* stream, ghc_tune
   };
   std::vector<Cand> cand;
   const bool mixed = prec == GHC_PREC_MIXED;
-  for (int f = 1; f >= (pb.N > 16 ? 1 : 0); --f)
+  const bool balanced = pb.hx_off[(size_t)pb.N * pb.N + 1] != kNoLanes;
+  for (int f = balanced ? 2 : 1; f >= (pb.N > 16 ? 1 : 0); --f)
     for (int v = 0; v < 2; ++v)
       for (int w = 0; w < (mixed ? 2 : 1); ++w) cand.push_back({v, mixed ? w : v, f});
   const int keep_v[2] = {pb.tune_variant[0], pb.tune_variant[1]};

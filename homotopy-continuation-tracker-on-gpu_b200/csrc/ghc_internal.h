@@ -34,6 +34,8 @@ constexpr int kMaxVarsPerTerm = 7;
 //   bits 11..16  PH : parameter index a ; bits 17..22 PH: parameter index b
 //   bit  23      H_x terms: the last term of its entry (row, column)
 //   bits 24..58  variable indices, 5 bits each, table order
+//   bits 49..58  words of the balanced H_x walk (at most 5 variable slots): the entry's row
+//                (49..53) and its slot among the row's non-zero entries (54..58)
 //   bits 59..63  H_x terms: the Jacobian column of the term (its row is implied by the CSR row)
 GHC_HD inline int term_scale(uint64_t w) { return (int)(int8_t)(w & 0xffu); }
 GHC_HD inline int term_nv(uint64_t w) { return (int)((w >> 8) & 7u); }
@@ -44,13 +46,31 @@ GHC_HD inline int term_var(uint64_t w, int q) { return (int)((w >> (24 + 5 * q))
 GHC_HD inline int term_col(uint64_t w) { return (int)(w >> 59); }
 constexpr uint64_t kTermLast = 1ull << 23;
 GHC_HD inline bool term_last(uint64_t w) { return (w & kTermLast) != 0; }
+GHC_HD inline int term_dst_row(uint64_t w) { return (int)((w >> 49) & 31u); }
+GHC_HD inline int term_dst_slot(uint64_t w) { return (int)((w >> 54) & 31u); }
+constexpr int kMaxVarsBalanced = 5;
 
-// Whether the tracker should walk each H_x row as one term list (staging the
-// entries in shared memory) rather than entry by entry.  Entry by entry, a
-// sub-warp runs, for every column, as many iterations as the row with the most
-// terms in that column; row-wise it runs as many as the longest row.  Above
-// 16 unknowns the kernels always walk rows (entry-wise code would be unrolled
-// N times).  hx_off: CSR offsets [N*N+1] of the compiled H_x terms.
+// lanes per path (the sub-warp width) for N unknowns
+GHC_HD constexpr int subwarp_width(int N) { return N <= 4 ? 4 : N <= 8 ? 8 : N <= 16 ? 16 : 32; }
+
+// Sizes that get the balanced H_x walk (tables and kernel code).  B200, tuned: 5-point (N = 6)
+// +11 %, 30x30 (N = 30) +4 %; at N = 12 both shipped problems ran 4-5 % slower even on the
+// row-wise walk once the balanced code and its tables were in the kernel, so it is left out there.
+GHC_HD constexpr bool balanced_walk_built(int N) { return N <= 8 || N > 16; }
+
+// The compiled H_x offsets: [N*N+1] CSR offsets of the terms per (row, column), then the
+// balanced walk: [1] its first word in the term array (kNoLanes: no balanced walk) and
+// [W] the number of terms each lane walks.
+constexpr uint16_t kNoLanes = 0xffff;
+GHC_HD constexpr int hx_off_len(int N) { return N * N + 2 + subwarp_width(N); }
+
+// The H_x walk the tracker should use by default: 0 entry by entry, 1 each lane its
+// row as one term list (staging the entries in shared memory), 2 the entries dealt
+// to all lanes balanced by term count.  Entry by entry, a sub-warp runs, for every
+// column, as many iterations as the row with the most terms in that column;
+// row-wise as many as the longest row; balanced as many as the longest lane.
+// Above 16 unknowns the kernels never walk entry by entry (that code would be
+// unrolled N times).  hx_off: the compiled H_x offsets (hx_off_len(N) entries).
 // The most structurally non-zero entries in one row of H_x: the row-wise walk stages each
 // row's non-zero entries in that many shared-memory slots.
 inline int row_nonzeros_max(const uint16_t* hx_off, int N) {
@@ -64,10 +84,22 @@ inline int row_nonzeros_max(const uint16_t* hx_off, int N) {
 }
 
 inline int flat_eval_pays(const uint16_t* hx_off, int N) {
-  int longest = 0, per_entry = 0;
+  int longest = 0, per_entry = 0, walk = 1;
   for (int r = 0; r < N; ++r) {
     const int len = hx_off[r * N + N] - hx_off[r * N];
     if (len > longest) longest = len;
+  }
+  if (hx_off[N * N + 1] != kNoLanes) {
+    // the balanced walk moves the same shared-memory traffic onto more lanes and adds a
+    // sub-warp synchronisation: by default only where the rows are uneven (longest row at
+    // least 1.4x the longest lane; the autotuner times it everywhere it is built)
+    int lane = 0;
+    for (int l = 0; l < subwarp_width(N); ++l)
+      if (hx_off[N * N + 2 + l] > lane) lane = hx_off[N * N + 2 + l];
+    if (10 * longest >= 14 * lane) {
+      longest = lane;
+      walk = 2;
+    }
   }
   for (int i = 0; i < N; ++i) {
     int m = 0;
@@ -77,7 +109,7 @@ inline int flat_eval_pays(const uint16_t* hx_off, int N) {
     }
     per_entry += m;
   }
-  return 4 * per_entry > 5 * longest ? 1 : 0;
+  return 4 * per_entry > 5 * longest ? walk : 0;
 }
 
 // Term shape of a problem: (variable slots per H_x term, per H_t term).  Every term of a
@@ -98,7 +130,7 @@ struct TrackParams {
   int kind, N, P, M, K;
   int max_steps, max_corr, incr;
   int n_hx_terms, n_ht_terms;
-  int flat_eval;              // walk H_x rows (flat_eval_pays() of the tables, or the autotuner's choice)
+  int flat_eval;              // H_x walk: 0 entry-wise, 1 row-wise, 2 balanced (flat_eval_pays() or the autotuner)
   int shape;                  // eval_shape_of() of the problem
   int scr_slots;              // row_nonzeros_max() of the tables
   int variant;                // compiled register-budget variant (0 or 1)

@@ -215,8 +215,53 @@ int compile_tables(const std::vector<int32_t>& hx, const std::vector<int32_t>& h
         out[(size_t)(k - off[(size_t)r * per_row]) * N + r] = terms[k];
     terms.swap(out);
   };
+  // Balanced H_x walk: the entries (row, column) are dealt to the W lanes of a sub-warp, longest
+  // first, each to the lane with the fewest terms so far (lowest lane on ties); a lane walks its
+  // entries' terms, each entry's in table order, so every sum is formed exactly as in the row-wise
+  // walk, only by another lane.  Words carry the entry's destination (row, slot among the row's
+  // non-zero entries).  Stored after the row-interleaved block, term q of lane l at q * W + l.
+  const int W = subwarp_width(N);
+  std::vector<uint64_t> lane_words;
+  std::vector<int> lane_len(W, 0);
+  const bool balanced = balanced_walk_built(N) && Px - 1 - n_coef_slots <= kMaxVarsBalanced;
+  if (balanced) {
+    struct Entry {
+      int r, slot, beg, end;
+    };
+    std::vector<Entry> entries;
+    for (int r = 0; r < N; ++r) {
+      int slot = 0;
+      for (int i = 0; i < N; ++i) {
+        const int beg = hx_off[(size_t)r * N + i], end = hx_off[(size_t)r * N + i + 1];
+        if (end > beg) entries.push_back({r, slot++, beg, end});
+      }
+    }
+    std::stable_sort(entries.begin(), entries.end(),
+                     [](const Entry& a, const Entry& b) { return a.end - a.beg > b.end - b.beg; });
+    std::vector<std::vector<int>> lists(W);
+    for (int e = 0; e < (int)entries.size(); ++e) {
+      int best = 0;
+      for (int l = 1; l < W; ++l)
+        if (lane_len[l] < lane_len[best]) best = l;
+      lists[best].push_back(e);
+      lane_len[best] += entries[e].end - entries[e].beg;
+    }
+    const int longest = *std::max_element(lane_len.begin(), lane_len.end());
+    lane_words.assign((size_t)longest * W, 0);
+    for (int l = 0; l < W; ++l) {
+      int q = 0;
+      for (int e : lists[l]) {
+        const Entry& en = entries[e];
+        for (int j = en.beg; j < en.end; ++j)
+          lane_words[(size_t)(q++) * W + l] = hx_terms[j] | (uint64_t)en.r << 49 | (uint64_t)en.slot << 54;
+      }
+    }
+  }
   interleave(hx_terms, hx_off, N);
   interleave(ht_terms, ht_off, 1);
+  hx_off.push_back(balanced ? (uint16_t)hx_terms.size() : kNoLanes);
+  for (int l = 0; l < W; ++l) hx_off.push_back((uint16_t)lane_len[l]);
+  hx_terms.insert(hx_terms.end(), lane_words.begin(), lane_words.end());
   if (hx_terms.size() > 60000 || ht_terms.size() > 60000) {
     set_error("too many terms");
     return GHC_ERR_LIMIT;

@@ -189,18 +189,24 @@ __device__ __forceinline__ cx<R> term_coef_value(uint64_t w, const cx<R>* ca) {
 // staged in the sub-warp's scratch slot scr[k][r] (only as many slots as the
 // fullest row has non-zero entries) and read back into registers through the
 // lane's non-zero mask nz (entry i is in slot popc(nz & (2^i - 1))); every slot
-// below the row's count is rewritten by every evaluation.  Entry-wise: one loop
-// per column, straight into registers.  Either way every entry is summed in
+// below the row's count is rewritten by every evaluation.  Balanced (walk 2): the
+// entries are dealt to all W lanes at table-compile time by term count, a lane
+// stores each finished sum into its row's slot, and the rows read their slots back
+// after a sub-warp synchronisation (max over lanes instead of over rows: 65 -> 43
+// iterations for the 5-point problem, whose rows hold 4..65 terms).  Entry-wise:
+// one loop per column, straight into registers.  Every walk sums each entry in
 // table order, as in the oracle.
 template <int N>
 constexpr bool kFlatAlways = N > 16;
 
 template <typename R, int N, int W, int KIND, int NVX, int NVT>
 __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, const cx<R>* cb, const cx<R>* xs, int r,
-                                         bool live, cx<R> (&A)[N], cx<R>& b, int which, bool flat,
+                                         bool live, cx<R> (&A)[N], cx<R>& b, int which, int walk,
                                          unsigned char* scr, unsigned nz) {
   auto slot = [&](int k) -> cx<R>* { return view<R>(scr) + (k * W + r); };
-  if (!kFlatAlways<N> && !flat) {
+  const int lanes = balanced_walk_built(N) ? tb.hx_off[N * N + 1] : kNoLanes;
+  const bool balanced = balanced_walk_built(N) && walk == 2 && lanes != kNoLanes;
+  if (!kFlatAlways<N> && walk == 0) {
 #pragma unroll
     for (int i = 0; i < N; ++i) {
       cx<R> acc = mk(R(0), R(0));
@@ -213,6 +219,23 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
       }
       A[i] = acc;
     }
+  } else if (balanced) {
+    // this lane's share of the entries (every lane of the sub-warp takes part); each finished
+    // sum goes into the slot of its row, read back after the sub-warp synchronises
+    const int len = tb.hx_off[N * N + 2 + r];
+    cx<R> acc = mk(R(0), R(0));
+    for (int q = 0; q < len; ++q) {
+      const uint64_t w = tb.hx_terms[lanes + q * W + r];
+      acc = acc_term<R, NVX>(acc, term_coef_value<R, KIND>(w, ca), w, xs);
+      if (term_last(w)) {
+        view<R>(scr)[term_dst_slot(w) * W + term_dst_row(w)] = acc;
+        acc = mk(R(0), R(0));
+      }
+    }
+    __syncwarp(kFull);  // other lanes wrote this row's slots
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+      A[i] = ((nz >> i) & 1u) ? *slot(__popc(nz & ((1u << i) - 1u))) : mk(R(0), R(0));
   } else {
     if (live) {
       const int len = tb.hx_off[r * N + N] - tb.hx_off[r * N];
@@ -227,6 +250,8 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
         }
       }
     }
+    // row-wise: this lane's own slots (each walk reads back inside its own branch: a read-back
+    // shared by the walks after the branches cost hundreds of bytes of register spills)
 #pragma unroll
     for (int i = 0; i < N; ++i)
       A[i] = ((nz >> i) & 1u) ? *slot(__popc(nz & ((1u << i) - 1u))) : mk(R(0), R(0));
@@ -448,6 +473,7 @@ struct SubMem {
   unsigned char* scr;    // H_x row scratch [slots][W], null unless the evaluation is flat
   unsigned char* rec;    // the path's scalar state while the sub-warp evaluates and solves [kRecBytes]
   unsigned nz;           // this lane's row: bit i set when H_x entry (row, i) has terms
+  int walk;              // H_x walk: 0 entry-wise, 1 row-wise, 2 balanced
 };
 constexpr int kRecBytes = 128;
 
@@ -466,7 +492,7 @@ template <typename R, int N, int W, int KIND, int S>
 __device__ __forceinline__ void eval_any(const Tables& tb, const SubMem& sm, int l, cx<R> (&A)[N], cx<R>& b,
                                          int which) {
   eval_row<R, N, W, KIND, shape_nvx(S), shape_nvt(S)>(tb, view<R>(sm.coefA), view<R>(sm.coefB), view<R>(sm.xs), l,
-                                                      l < N, A, b, which, sm.scr != nullptr, sm.scr, sm.nz);
+                                                      l < N, A, b, which, sm.walk, sm.scr, sm.nz);
 }
 
 // one evaluation + solve in precision R; returns this lane's solution component
@@ -501,7 +527,7 @@ __device__ __forceinline__ void coef_eval(const TrackParams& p, const SubMem& sm
 // byte sizes of the shared-memory layout
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 __host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
-  return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(N * N + 1 + N + 1));
+  return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(hx_off_len(N) + N + 1));
 }
 // per sub-warp: the path record [kRecBytes], then in complex values of esz bytes: coefficient
 // buffers [2 Mc], track [N+1], two pivot rows [2 (N+1)], solution [N], lane state [2 W], scratch
@@ -559,10 +585,10 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
   uint64_t* s_hx = reinterpret_cast<uint64_t*>(smem);
   uint64_t* s_ht = s_hx + n_hx;
   uint16_t* s_hxo = reinterpret_cast<uint16_t*>(s_ht + n_ht);
-  uint16_t* s_hto = s_hxo + N * N + 1;
+  uint16_t* s_hto = s_hxo + hx_off_len(N);
   for (int i = threadIdx.x; i < n_hx; i += blockDim.x) s_hx[i] = __ldg(g_hx + i);
   for (int i = threadIdx.x; i < n_ht; i += blockDim.x) s_ht[i] = __ldg(g_ht + i);
-  for (int i = threadIdx.x; i < N * N + 1; i += blockDim.x) s_hxo[i] = __ldg(g_hxo + i);
+  for (int i = threadIdx.x; i < hx_off_len(N); i += blockDim.x) s_hxo[i] = __ldg(g_hxo + i);
   for (int i = threadIdx.x; i < N + 1; i += blockDim.x) s_hto[i] = __ldg(g_hto + i);
   __syncthreads();
   Tables t;
@@ -603,11 +629,13 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
   const int l = lane % W;
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
-  const bool flat = kFlatAlways<N> || p.flat_eval;
+  const int walk = (kFlatAlways<N> && p.flat_eval == 0) ? 1 : p.flat_eval;
+  const bool flat = walk != 0;
   SubMem sm = sub_layout<R>(smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) +
                                 (size_t)g * sub_bytes(N, Mc, W, flat ? p.scr_slots : 0, (int)sizeof(cx<R>)),
                             N, Mc, W, flat);
   sm.nz = row_mask<N>(tb.hx_off, l);
+  sm.walk = walk;
   // this lane's RK base point x0 and accumulator sols live in shared memory (register relief)
   cx<R>& x0 = view<R>(sm.state)[l];
   cx<R>& sols = view<R>(sm.state)[W + l];
@@ -871,11 +899,13 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
   const int l = lane % W;
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
-  const bool flat = kFlatAlways<N> || p.flat_eval;
+  const int walk = (kFlatAlways<N> && p.flat_eval == 0) ? 1 : p.flat_eval;
+  const bool flat = walk != 0;
   SubMem sm = sub_layout<double>(
       smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, W, flat ? p.scr_slots : 0, 16),
       N, Mc, W, flat);
   sm.nz = row_mask<N>(tb.hx_off, l);
+  sm.walk = walk;
   const int subs_per_cta = blockDim.x / W;
   const int leader = lane - l;
   for (long long item0 = (long long)blockIdx.x * subs_per_cta; item0 < p.n_items;

@@ -236,6 +236,8 @@ def autotune(pb, ws, d_start_sols, **kw):
 
 
 def set_tuning(pb, precision, variant, flat=-1):
+    """Launch choice for ``precision``: register-budget ``variant`` (0, 1) and H_x walk ``flat``
+    (0 entry-wise, 1 row-wise, 2 balanced over all lanes, -1 from the table structure)."""
     _check(ghc_set_tuning(pb.h, precision, variant, flat), "ghc_set_tuning")
 
 

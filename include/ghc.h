@@ -166,8 +166,10 @@ int ghc_track_noalloc(const ghc_problem* pb, const ghc_track_args* args, void* s
  *   variant  the compiled register budget (0: the default table of CTAs per SM,
  *            1: one more CTA per SM with fewer registers per thread);
  *   flat     how H_x is walked (1: each lane walks its row once through a
- *            shared-memory scratch row, 0: one loop per column; -1: chosen from
- *            the table structure; above 16 unknowns always 1).
+ *            shared-memory scratch row, 2: the entries are dealt to all lanes
+ *            of the sub-warp balanced by term count, each sum stored into its
+ *            row's scratch slot, 0: one loop per column; -1: chosen from the
+ *            table structure; above 16 unknowns 1 or 2).
  * Every choice computes bit-identical results; only the speed differs.
  *
  * ghc_autotune runs the caller's sample batch (`sample`, exactly as for

@@ -70,7 +70,7 @@ def test_mixed_server_and_tuning_keep_results():
         assert np.array_equal(e[fin], r.endpoints[fin])
     tuned = serve.Server(torch, problems=["P3P_TD"], max_batch=512, tune=True)
     plain = serve.Server(torch, problems=["P3P_TD"], max_batch=512)
-    assert tuned.problems["P3P_TD"].tuning["candidates"] == 4
+    assert tuned.problems["P3P_TD"].tuning["candidates"] == 6  # 2 register budgets x 3 H_x walks
     _, _, _, rt = serve.run_stream(tuned, lam=5000, n_req=5, seed=9)
     _, _, _, rp = serve.run_stream(plain, lam=5000, n_req=5, seed=9)
     for x, y in zip(rt, rp):

@@ -158,6 +158,8 @@ def test_tuning_setters_validate():
     assert ghc.get_tuning(pb, ghc.PREC_FP64) == (1, 0) and ghc.get_tuning(pb, ghc.PREC_FP32) == (1, 0)
     ghc.set_tuning(pb, ghc.PREC_FP32, 0, 1)
     assert ghc.get_tuning(pb, ghc.PREC_FP64) == (1, 0) and ghc.get_tuning(pb, ghc.PREC_FP32) == (0, 1)
-    for bad in [(ghc.PREC_FP64, 2, 0), (ghc.PREC_FP64, 0, 2), (7, 0, 0)]:
+    ghc.set_tuning(pb, ghc.PREC_FP64, 0, 2)
+    assert ghc.get_tuning(pb, ghc.PREC_FP64) == (0, 2)
+    for bad in [(ghc.PREC_FP64, 2, 0), (ghc.PREC_FP64, 0, 3), (ghc.PREC_FP64, 0, -2), (7, 0, 0)]:
         with pytest.raises(ghc.GhcError):
             ghc.set_tuning(pb, *bad)

@@ -342,6 +342,24 @@ int ghc_problem_raw_tables(const ghc_problem* h, int32_t* hx, int32_t* ht) {
   return GHC_OK;
 }
 
+int ghc_problem_compiled_tables(const ghc_problem* h, uint64_t* words, int32_t words_cap, uint16_t* off,
+                                int32_t off_cap, int32_t* n_words, int32_t* n_off) {
+  if (!h || !n_words || !n_off) {
+    set_error("null argument");
+    return GHC_ERR_ARG;
+  }
+  const Problem& pb = h->pb;
+  *n_words = (int32_t)pb.hx_terms.size();
+  *n_off = (int32_t)pb.hx_off.size();
+  if ((words && words_cap < *n_words) || (off && off_cap < *n_off)) {
+    set_error("buffer smaller than the compiled tables");
+    return GHC_ERR_LIMIT;
+  }
+  if (words) std::memcpy(words, pb.hx_terms.data(), pb.hx_terms.size() * sizeof(uint64_t));
+  if (off) std::memcpy(off, pb.hx_off.data(), pb.hx_off.size() * sizeof(uint16_t));
+  return GHC_OK;
+}
+
 int ghc_p2c(const ghc_problem* h, const double* start, const double* target, double* hx, double* ht, int exact_ht) {
   if (!h || !start || !target || !hx || !ht) {
     set_error("null argument");

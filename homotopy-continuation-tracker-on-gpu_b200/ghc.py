@@ -73,6 +73,7 @@ ghc_problem_get_info = _sig("ghc_problem_get_info", ctypes.c_int, [_P, ctypes.PO
 ghc_problem_start_sols = _sig("ghc_problem_start_sols", ctypes.c_int, [_P, _P])
 ghc_problem_params = _sig("ghc_problem_params", ctypes.c_int, [_P, _P, _P])
 ghc_problem_raw_tables = _sig("ghc_problem_raw_tables", ctypes.c_int, [_P, _P, _P])
+ghc_problem_compiled_tables = _sig("ghc_problem_compiled_tables", ctypes.c_int, [_P, _P, _I32, _P, _I32, _P, _P])
 ghc_p2c = _sig("ghc_p2c", ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int])
 ghc_p2c_device = _sig("ghc_p2c_device", ctypes.c_int, [_P, _I64, _P, _P, _P, _P, ctypes.c_int, _P])
 ghc_track = _sig("ghc_track", ctypes.c_int, [_P, ctypes.POINTER(TrackArgs), _P])
@@ -163,6 +164,17 @@ class Problem:
         ht = np.zeros(self.N * self.Tt * self.Pt, dtype=np.int32)
         _check(ghc_problem_raw_tables(self.h, hx.ctypes.data, ht.ctypes.data), "ghc_problem_raw_tables")
         return hx, ht
+
+    def compiled_hx(self):
+        """The compiled H_x tables the tracker walks: (uint64 term words, uint16 offsets)."""
+        nw, no = _I32(), _I32()
+        _check(ghc_problem_compiled_tables(self.h, None, 0, None, 0, ctypes.byref(nw), ctypes.byref(no)),
+               "ghc_problem_compiled_tables")
+        w = np.zeros(nw.value, dtype=np.uint64)
+        o = np.zeros(no.value, dtype=np.uint16)
+        _check(ghc_problem_compiled_tables(self.h, w.ctypes.data, nw.value, o.ctypes.data, no.value,
+                                           ctypes.byref(nw), ctypes.byref(no)), "ghc_problem_compiled_tables")
+        return w, o
 
     def p2c(self, start, target, exact_ht=False):
         """Host coefficient tables for one hypothesis -> (hx [(M+1)(K+1)], ht [(M+1)K]) complex."""

@@ -81,6 +81,14 @@ int ghc_problem_start_sols(const ghc_problem* pb, double* h_out);
 int ghc_problem_params(const ghc_problem* pb, double* h_start, double* h_target);
 /* raw tables as read: h_hx [N*N*Tx*Px], h_ht [N*Tt*Pt] */
 int ghc_problem_raw_tables(const ghc_problem* pb, int32_t* h_hx, int32_t* h_ht);
+/* The compiled H_x tables the tracker walks (for inspection): *n_words 64-bit term words (the
+ * row-interleaved block: term k of row r at k*N + r; then the balanced walk's block: term q of
+ * lane l at first + q*W + l) and *n_off 16-bit offsets (N*N+1 CSR offsets per (row, column),
+ * the balanced block's first word or 0xffff when the size has no balanced walk, W lane lengths).
+ * Copies when h_words / h_off are non-null and hold *n_words / *n_off entries (GHC_ERR_LIMIT if
+ * the capacities are smaller); null buffers only return the sizes. */
+int ghc_problem_compiled_tables(const ghc_problem* pb, uint64_t* h_words, int32_t words_cap, uint16_t* h_off,
+                                int32_t off_cap, int32_t* n_words, int32_t* n_off);
 
 /* ---------------------------------------------------------------------------
  * Coefficient homotopy tables (P2C problems).

@@ -111,6 +111,24 @@ def test_error_table_index_out_of_range(tmp_path):
         ghc.Problem("P3P", root=str(tmp_path))
 
 
+def test_error_term_scale_outside_int8(tmp_path):
+    d = _copy_problem(tmp_path)
+    vals = open(d / "dHdx_indx.txt").read().split()
+    vals[0] = "300"  # the first term's integer scale: the term word holds it in 8 bits
+    open(d / "dHdx_indx.txt", "w").write(" ".join(vals))
+    with pytest.raises(ghc.GhcError, match=r"\(-4\).*int8"):
+        ghc.Problem("P3P", root=str(tmp_path))
+
+
+def test_error_variable_index_out_of_range(tmp_path):
+    d = _copy_problem(tmp_path)
+    vals = open(d / "dHdx_indx.txt").read().split()
+    vals[2] = "9"  # the first term's variable slot: beyond N (slot N = 3 is the constant 1)
+    open(d / "dHdx_indx.txt", "w").write(" ".join(vals))
+    with pytest.raises(ghc.GhcError, match=r"\(-4\).*variable"):
+        ghc.Problem("P3P", root=str(tmp_path))
+
+
 def test_error_truncated_table(tmp_path):
     d = _copy_problem(tmp_path)
     vals = open(d / "dHdt_indx.txt").read().split()

@@ -183,7 +183,7 @@ def reference_arm(args, rank):
     import oracle as O
     import scenes
     ob = O.Problem(PROBLEM)
-    sample = 8
+    sample = 32
     cores = os.cpu_count() or 1
     tg, _ = scenes.generalized_3views_4pts(sample * (args.steps + args.warmup), seed=1000 + args.seed)
     times = []
@@ -203,7 +203,7 @@ def reference_arm(args, rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
             "data": "synthetic (seeded scenes)", "config": workload_config(args.hyp),
             "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "cpu_model": cpu_model(),
                              "sample": "%d hypotheses x 583 paths per step, %d steps" % (sample, len(times))},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -317,10 +317,13 @@ def main():
 
     extra = {}
     if rank == 0:
+        # parity and recall against the oracle on the bench's own scenes: the first S hypotheses of
+        # the timed batch, tracked again with the FP64 polish (untimed) and by the oracle
+        extra["oracle_check"], cpu = oracle_check(args, pb, ghc, d_start, d_tg, d_sols, tg, ws, H)
         # recall of the batched run vs single-hypothesis drop-in launches of the same hypotheses
         n_chk = min(H, 16)
         ws1 = ghc.Workspace(pb, 1, ghc.PREC_FP64)
-        real_b = real_s = match = 0
+        real_s = match = 0
         single_ms = []
         for h in range(n_chk):
             torch.cuda.synchronize()
@@ -339,7 +342,6 @@ def main():
             for e in e1s[rs]:
                 d = np.abs(blk[cb] - e).max(axis=1) / max(1.0, np.abs(e).max())
                 match += bool(d.size and d.min() <= 1e-8)
-            real_b += int((cb & (np.abs(blk.imag).max(axis=1) <= 1e-8)).sum())
         extra["recall_vs_single_hypothesis_fp64"] = match / max(1, real_s)
         extra["dropin_single_hypothesis"] = {"value": 1e3 / statistics.median(single_ms), "unit": UNIT,
                                              "note": "one hypothesis per launch, median wall ms %.3f"
@@ -373,36 +375,43 @@ def main():
                             "ms_h2d_solve_d2h": [float(v) for v in split],
                             "path": "ghc_solve_host (C ABI, pinned host buffers, synchronous, one call per step)"}
             assert np.array_equal(out["conv"], conv), "e2e run differs from the timed run"
-            extra["cpu_baseline"] = cpu_baseline(args)
+            extra["cpu_baseline"] = cpu
     clocks_sum = clocks.summary()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return
+    # algorithmic bytes of one tracker launch: the per-hypothesis coefficient tables and the shared
+    # start solutions in; endpoints, three flag bytes, step / corrector counts, t_end and dt_end out
+    n_items = H * pb.paths
+    alg_bytes = (H * ((pb.M + 1) * (pb.K + 1) + (pb.M + 1) * pb.K) * 16 + pb.paths * pb.N * 16 +
+                 n_items * (pb.N * 16 + 3 + 4 + 4 + 8 + 8))
     traffic = None
     tp = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tp):
         t = json.load(open(tp)).get(PROBLEM)
-        if t:
-            traffic = t["bytes_per_path"] * H * pb.paths
+        if t and t.get("hypotheses"):
+            # DRAM bytes of one full-size launch (ncu, read + write), scaled by the hypotheses tracked
+            traffic = t["dram_bytes_per_launch"] * H / t["hypotheses"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": n_steps, "warmup": args.warmup,
         "ms_per_step": total_ms / n_steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "complex128", "data": "synthetic (seeded scenes)", "config": workload_config(H),
         "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
-        "recall": extra.get("recall_vs_single_hypothesis_fp64"),
+        "recall": (extra.get("oracle_check") or {}).get("recall_vs_oracle"),
         "paths": {"per_step": H * pb.paths, "converged_frac": float(conv.mean()), "mean_steps": float(steps.mean()),
                   "mean_corrector_iters": float(corr.mean())},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
-                     "frac": achieved / peak64, "traffic": traffic,
+                     "frac": achieved / peak64, "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
                      "peak_source": "measured FP64 FMA throughput (ghc_measure_fma_peak, burst)",
                      "kernel_ms": kern_avg_ms, "algorithmic_flop_per_launch": flops_launch},
         "clocks": clocks_sum,
         "tuning": tuning,
         "gpu_launches": 2 * n_steps,
     }
-    for k in ("e2e", "cpu_baseline", "modes", "dropin_single_hypothesis"):
+    for k in ("e2e", "cpu_baseline", "oracle_check", "recall_vs_single_hypothesis_fp64", "modes",
+              "dropin_single_hypothesis"):
         if k in extra:
             line[k] = extra[k]
     print(json.dumps(line), flush=True)
@@ -462,22 +471,89 @@ def secondary_modes(pb, ghc, cx, d_start, d_sols, scenes, dev, args):
     return out
 
 
-def cpu_baseline(args):
-    """The oracle (CPU restatement of the reference tracker) on a bounded sample, all host cores."""
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def real_mask(e, conv, resid):
+    """Real solutions of the recall definition: converged, every |Im| <= 1e-8 and |H(x, 1)| < 1e-10
+    after the FP64 polish."""
+    return (conv == 1) & (np.abs(e.imag).max(axis=1) <= 1e-8) & (resid >= 0) & (resid < 1e-10)
+
+
+def recall_and_error(e_ref, c_ref, r_ref, e_c, c_c, paths):
+    """Share of the reference run's real solutions that the candidate run finds within 1e-8
+    (max-norm, relative to max(1, |x|)), hypothesis by hypothesis, and the error of every matched
+    endpoint (max and 99th percentile)."""
+    real = real_mask(e_ref, c_ref, r_ref)
+    found, errs = 0, []
+    for i in np.nonzero(real)[0]:
+        h = i // paths
+        cand = e_c[h * paths:(h + 1) * paths][c_c[h * paths:(h + 1) * paths] == 1]
+        d = np.abs(cand - e_ref[i]).max(axis=1) / max(1.0, np.abs(e_ref[i]).max()) if cand.size else np.array([np.inf])
+        errs.append(float(d.min()))
+        found += bool(d.min() <= 1e-8)
+    errs = np.array(errs) if errs else np.zeros(1)
+    fin = errs[errs <= 1e-8]
+    return (found / max(1, int(real.sum())), int(real.sum()),
+            {"max": float(fin.max()) if fin.size else None,
+             "p99": float(np.percentile(fin, 99)) if fin.size else None})
+
+
+def oracle_check(args, pb, ghc, d_start, d_tg, d_sols, tg, ws, H):
+    """The GPU batch against the oracle on the bench's own first S scenes.
+
+    Flags and counters of the timed (unpolished) run, and the endpoints and residuals of the same
+    hypotheses tracked again with 3 FP64 polish iterations, must equal the oracle's bit for bit;
+    recall = the share of the oracle's real solutions that the GPU finds within 1e-8.  The oracle
+    run, on all host cores, is also the CPU baseline, plus a 1-core run on a smaller sample."""
+    import torch
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as O
-    import scenes
+    S = min(H, 128)
+    n = pb.paths
+    ws_p = ghc.Workspace(pb, S, ghc.PREC_FP64)
+    hx, ht = pb.p2c_device(d_start, d_tg[:S])
+    ghc.track(pb, ws_p, d_sols, d_coef_hx=hx, d_coef_ht=ht, polish_iters=3, want_resid=True)
+    torch.cuda.synchronize()
+    g = {k: getattr(ws_p, k).cpu().numpy() for k in ("conv", "inf", "status", "steps", "corr", "resid")}
+    ge = ws_p.endpoints.cpu().numpy()
+    ge = ge[..., 0] + 1j * ge[..., 1]
     ob = O.Problem(PROBLEM)
+    ohx = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[0] for t in tg[:S]])
+    oht = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[1] for t in tg[:S]])
     cores = os.cpu_count() or 1
-    sample = 8
-    tg, _ = scenes.generalized_3views_4pts(sample, seed=77 + args.seed)
-    hx = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[0] for t in tg])
-    ht = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[1] for t in tg])
     t0 = time.perf_counter()
-    O.track(ob, ob.start_sols, hx=hx, ht=ht, nthreads=cores)
-    dt = time.perf_counter() - t0
-    return {"value": sample / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "%d hypotheses x 583 paths (same scene generator), FP64, reference step control" % sample}
+    r = O.track(ob, ob.start_sols, hx=ohx, ht=oht, polish_iters=3, nthreads=cores)
+    dt_all = time.perf_counter() - t0
+    s1 = 4
+    t0 = time.perf_counter()
+    O.track(ob, ob.start_sols, hx=ohx[:s1], ht=oht[:s1], polish_iters=3, nthreads=1)
+    dt_one = time.perf_counter() - t0
+    timed = {k: getattr(ws, k)[:S * n].cpu().numpy() for k in ("conv", "inf", "status", "steps", "corr")}
+    same = {k: bool(np.array_equal(g[k], r[k])) for k in ("conv", "inf", "status", "steps", "corr")}
+    same["timed_run_flags_and_counters"] = all(bool(np.array_equal(timed[k], r[k])) for k in timed)
+    fin = np.isfinite(r["endpoints"])
+    same["endpoints"] = bool(np.array_equal(np.isfinite(ge), fin) and np.array_equal(ge[fin], r["endpoints"][fin]))
+    cv = r["conv"] == 1
+    same["residuals"] = bool(np.array_equal(g["resid"][cv], r["resid"][cv]))
+    rec, n_real, err = recall_and_error(r["endpoints"], r["conv"], r["resid"], ge, g["conv"], n)
+    check = {"hypotheses": S, "paths": S * n, "bit_exact": all(same.values()), "equal": same,
+             "recall_vs_oracle": rec, "oracle_real_solutions": n_real, "endpoint_error_vs_oracle": err,
+             "definition": "real = converged, |Im| <= 1e-8, |H(x,1)| < 1e-10 after 3 FP64 polish iterations; "
+                           "found = a converged GPU endpoint of the same hypothesis within 1e-8 (max-norm, "
+                           "relative to max(1, |x|))"}
+    cpu = {"value": S / dt_all, "unit": UNIT, "cores": cores, "kind": "port", "cpu_model": cpu_model(),
+           "sample": "the bench's own first %d scenes x %d paths, FP64, reference step control, 3 polish "
+                     "iterations (the oracle run the parity check above compares with)" % (S, n),
+           "one_core": {"value": s1 / dt_one, "unit": UNIT, "sample": "first %d of those scenes" % s1}}
+    return check, cpu
 
 
 if __name__ == "__main__":

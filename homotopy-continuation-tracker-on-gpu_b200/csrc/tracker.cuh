@@ -278,18 +278,20 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
   b = which ? mk(-h.re, -h.im) : h;
 }
 
-// Pivot key of a row for column i: magnitude |Re|+|Im| quantised to its upper
-// bits, position in the low 5 bits (largest key = largest magnitude, lowest
-// position among equal ones).  Pivoted rows 0; NaN at the current position
-// wins, NaN below never does (reference dev-cgesv-batched-small.cuh:54-65).
+// Pivot key of a row for column i: magnitude |Re|+|Im| cut to its upper bits, position in the
+// low 5 bits (largest key = largest cut magnitude, lowest position among equal ones).  Pivoted
+// rows 0; a NaN at the current position wins, a NaN below never does.  The cut only speeds up the
+// search: pivot_search resolves every near tie on the full magnitudes.
 __device__ __forceinline__ unsigned mag_bits(double v) { return (unsigned)__double2hiint(v); }
 __device__ __forceinline__ unsigned mag_bits(float v) { return __float_as_uint(v); }
 template <typename R>
 __device__ __forceinline__ unsigned pivot_key(R v, int pos, int i) {
   if (pos < i) return 0u;
-  if (v != v) return (pos == i) ? 0xffffffffu : 0u;
+  if (v != v) return (pos == i) ? (0xffffffe0u | (unsigned)(31 - pos)) : 0u;
   return ((mag_bits(v) >> 5) << 5) | (unsigned)(31 - pos);
 }
+__device__ __forceinline__ unsigned long long full_bits(double v) { return (unsigned long long)__double_as_longlong(v); }
+__device__ __forceinline__ unsigned long long full_bits(float v) { return (unsigned long long)__float_as_uint(v); }
 
 // compile-time loop: f(integral_constant<int, I>) for I in [B, E)
 template <int B, int E, typename F>
@@ -321,11 +323,47 @@ constexpr int LU_UNROLLED = 0, LU_ROLLED = 1;
 template <int N>
 constexpr int kLuForm = N <= 16 ? LU_UNROLLED : GHC_LU_LARGE;
 
+// Pivot position of column i, the reference's rule (dev-cgesv-batched-small.cuh:54-65): the
+// largest |Re|+|Im| among the unpivoted rows, the lowest position among equal magnitudes, a NaN
+// at position i kept and a NaN below never taken.  An integer max butterfly over pivot_key finds
+// it in one shuffle per level; that answer is exact unless another unpivoted row shares the
+// winner's cut magnitude, and then (in any sub-warp of the warp) the full magnitudes and the
+// positions are reduced as pairs.
 template <typename R, int W>
 __device__ __forceinline__ int pivot_search(cx<R> a, bool live, int pos, int i) {
-  unsigned best = live ? pivot_key(fabs(a.re) + fabs(a.im), pos, i) : 0u;
+  const R m = fabs(a.re) + fabs(a.im);
+  const unsigned key = live ? pivot_key(m, pos, i) : 0u;
+  unsigned best = key;
 #pragma unroll
   for (int off = W / 2; off > 0; off >>= 1) best = max(best, __shfl_xor_sync(kFull, best, off, W));
+  const bool cand = live && pos >= i;
+  const unsigned near = __ballot_sync(kFull, cand && ((key ^ best) >> 5) == 0u);
+  const unsigned mine = (W == 32) ? near : (near >> ((threadIdx.x & 31) & ~(W - 1))) & ((1u << (W & 31)) - 1u);
+  if (__any_sync(kFull, __popc(mine) > 1)) {
+    // (magnitude bits, position): non-negative magnitudes order as their bit patterns; a NaN at
+    // position i first, a NaN below and the pivoted rows last
+    unsigned long long mb = 0ull;
+    int mp = 64;
+    if (cand) {
+      if (m == m) {
+        mb = full_bits(m);
+        mp = pos;
+      } else if (pos == i) {
+        mb = ~0ull;
+        mp = pos;
+      }
+    }
+#pragma unroll
+    for (int off = W / 2; off > 0; off >>= 1) {
+      const unsigned long long ob = __shfl_xor_sync(kFull, mb, off, W);
+      const int op = __shfl_xor_sync(kFull, mp, off, W);
+      if (ob > mb || (ob == mb && op < mp)) {
+        mb = ob;
+        mp = op;
+      }
+    }
+    return mp;
+  }
   return 31 - (int)(best & 31u);
 }
 

@@ -94,6 +94,7 @@ ghc_kernel_HC_Solver_P2C_z = _sig("ghc_kernel_HC_Solver_P2C_z", ctypes.c_double,
 ghc_kernel_HC_Solver_PH = _sig("ghc_kernel_HC_Solver_PH", ctypes.c_double, _DROPIN_PH)
 ghc_kernel_HC_Solver_PH_z = _sig("ghc_kernel_HC_Solver_PH_z", ctypes.c_double, _DROPIN_PH)
 ghc_measure_fma_peak = _sig("ghc_measure_fma_peak", ctypes.c_int, [ctypes.c_int, _P, _P])
+ghc_lu_solve_device = _sig("ghc_lu_solve_device", ctypes.c_int, [_I32, _I32, _I64, _P, _P, _P, _P])
 
 
 class GhcError(RuntimeError):
@@ -290,6 +291,17 @@ def measure_fma_peak(precision=PREC_FP64):
     ms = ctypes.c_double()
     _check(ghc_measure_fma_peak(precision, ctypes.byref(f), ctypes.byref(ms)), "ghc_measure_fma_peak")
     return f.value
+
+
+def lu_solve_device(d_A, d_b, precision=PREC_FP64):
+    """The tracker's linear solve on the device: d_A [n, N, N, 2], d_b [n, N, 2] float64 (FP64) or
+    float32 (FP32) tensors -> d_z [n, N, 2] (torch's current stream)."""
+    import torch
+    n, N = d_A.shape[0], d_A.shape[1]
+    z = torch.empty_like(d_b)
+    _check(ghc_lu_solve_device(N, precision, n, d_A.data_ptr(), d_b.data_ptr(), z.data_ptr(), _stream()),
+           "ghc_lu_solve_device")
+    return z
 
 
 def count_results(endpoints, conv, inf, imag_tol=1e-4, dup_tol=1e-4):

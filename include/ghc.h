@@ -273,6 +273,19 @@ int ghc_solve_host(const ghc_problem* pb, int32_t precision, int64_t n_hyp, cons
  * ------------------------------------------------------------------------- */
 int ghc_measure_fma_peak(int precision, double* flops_per_s, double* ms);
 
+/* ---------------------------------------------------------------------------
+ * The tracker's linear solve on its own (diagnostics).  Replaces nothing callable:
+ * it runs the device LU that stands in for cgesv_batched_small_device
+ * (GPU-HC/magmaHC/dev-cgesv-batched-small.cuh:40-107) -- pivot = the largest |Re|+|Im|
+ * among the unpivoted rows, the lowest position on ties, a NaN at the current position
+ * kept and a NaN below never taken; a zero pivot skips its elimination -- on n_sys
+ * systems A z = b of N unknowns, one sub-warp per system, asynchronously on `stream`.
+ * d_A [n_sys][N][N] (row-major), d_b [n_sys][N], d_z [n_sys][N] complex: double pairs
+ * for GHC_PREC_FP64, float pairs for GHC_PREC_FP32.  N in {3,4,5,6,8,10,11,12,16,18,30}.
+ * ------------------------------------------------------------------------- */
+int ghc_lu_solve_device(int32_t N, int32_t precision, int64_t n_sys, const void* d_A, const void* d_b, void* d_z,
+                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif

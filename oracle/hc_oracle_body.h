@@ -32,9 +32,9 @@
  *   - padding terms (integer scale 0) are skipped (variable slot N, the
  *     constant 1, is multiplied in like any other slot, as in the reference);
  *   - the pivot reciprocal is conj(b)/|b|^2 (one reciprocal); the back
- *     substitution multiplies by the reciprocal formed during elimination;
- *   - pivot magnitudes are compared after quantisation to their upper bits
- *     (pivot_key), ties going to the lowest position.
+ *     substitution multiplies by the reciprocal formed during elimination.
+ * The pivot rule is the reference's own: strict argmax of |Re|+|Im| over the
+ * unpivoted positions in order (lowest position on ties).
  */
 
 #define CAT2(a, b) a##b
@@ -198,57 +198,41 @@ static CX SFX(eval_h_row)(const orc_problem* pb, const COEFS* cf, const CX* x, i
 }
 
 /*
- * Pivot key of one row for column i: the magnitude |Re|+|Im| quantised to its
- * upper bits with the position in the low 5 bits, so the largest key is the
- * largest magnitude and, among magnitudes equal after quantisation, the
- * lowest position.  Pivoted rows get 0; a NaN at the current position gets the
- * maximum (the reference keeps position i when its value is NaN), NaN below
- * never wins (its comparisons are false in the reference's scan).
- */
-static inline uint32_t SFX(pivot_key)(REAL v, int pos, int i) {
-  if (pos < i) return 0u;
-  if (v != v) return (pos == i) ? 0xffffffffu : 0u;
-  uint32_t hi;
-  if (sizeof(REAL) == 8) {
-    double d = (double)v;
-    uint64_t b;
-    memcpy(&b, &d, 8);
-    hi = (uint32_t)(b >> 32);
-  } else {
-    float f = (float)v;
-    memcpy(&hi, &f, 4);
-  }
-  return ((hi >> 5) << 5) | (uint32_t)(31 - pos);
-}
-
-/*
  * Solve A z = b with partial pivoting, one row per (virtual) lane.
- * Pivot: the row with the largest pivot_key among not-yet-pivoted rows.  A
- * zero pivot skips the elimination for that column and leaves a non-finite
- * solution, as in the reference.  The solution is returned in variable order.
+ * Pivot of column i: the reference's scan (GPU-HC/magmaHC/dev-cgesv-batched-small.cuh:54-65)
+ * over the positions i..N-1 in order, starting from position i and moving only to a strictly
+ * larger |Re|+|Im|: the largest magnitude, the lowest position among equal ones; a NaN at
+ * position i is kept, a NaN below is never taken.  A zero pivot skips the elimination for that
+ * column and leaves a non-finite solution, as in the reference.  The solution is returned in
+ * variable order.  trace (optional): piv[i] = the pivot position of column i, and
+ * mags[i*N + j] = |Re|+|Im| of the row at position j (j >= i) when column i was searched.
  */
-static void SFX(lu_solve)(int N, CX A[][ORC_NMAX], CX* b, CX* z) {
-  int pos[ORC_NMAX];
+static void SFX(lu_solve_trace)(int N, CX A[][ORC_NMAX], CX* b, CX* z, int32_t* piv, REAL* mags) {
+  int pos[ORC_NMAX], row_at[ORC_NMAX];
   CX myrcp[ORC_NMAX];
-  for (int r = 0; r < N; ++r) pos[r] = r;
+  for (int r = 0; r < N; ++r) pos[r] = row_at[r] = r;
   for (int i = 0; i < N; ++i) {
-    int best_r = -1;
-    uint32_t best_key = 0;
-    for (int r = 0; r < N; ++r) {
-      const uint32_t key = SFX(pivot_key)(FABS(A[r][i].re) + FABS(A[r][i].im), pos[r], i);
-      if (best_r < 0 || key > best_key) {
-        best_r = r;
-        best_key = key;
+    int best_pos = i;
+    REAL best = FABS(A[row_at[i]][i].re) + FABS(A[row_at[i]][i].im);
+    if (mags) mags[i * N + i] = best;
+    for (int j = i + 1; j < N; ++j) {
+      const REAL v = FABS(A[row_at[j]][i].re) + FABS(A[row_at[j]][i].im);
+      if (mags) mags[i * N + j] = v;
+      if (v > best) {
+        best = v;
+        best_pos = j;
       }
     }
-    const int best_pos = 31 - (int)(best_key & 31u);
-    for (int r = 0; r < N; ++r)
-      if (pos[r] == best_pos) best_r = r;
+    if (piv) piv[i] = best_pos;
+    const int best_r = row_at[best_pos];
     /* zero pivot: the pivot row's own magnitude is exactly 0 */
-    const int zero = (FABS(A[best_r][i].re) + FABS(A[best_r][i].im) == (REAL)0);
-    for (int r = 0; r < N; ++r)
-      if (r != best_r && pos[r] == i) pos[r] = best_pos;
+    const int zero = (best == (REAL)0);
+    /* the pivot row moves to position i, the row at position i to the pivot's position */
+    const int r_i = row_at[i];
+    pos[r_i] = best_pos;
+    row_at[best_pos] = r_i;
     pos[best_r] = i;
+    row_at[i] = best_r;
     CX sx[ORC_NMAX];
     for (int j = i; j < N; ++j) sx[j] = A[best_r][j];
     const CX sb = b[best_r];
@@ -264,9 +248,7 @@ static void SFX(lu_solve)(int N, CX A[][ORC_NMAX], CX* b, CX* z) {
     }
   }
   for (int i = N - 1; i >= 0; --i) {
-    int ri = 0;
-    for (int r = 0; r < N; ++r)
-      if (pos[r] == i) ri = r;
+    const int ri = row_at[i];
     const CX xi = SFX(c_mul)(b[ri], myrcp[ri]);
     for (int r = 0; r < N; ++r)
       if (pos[r] < i) b[r] = SFX(c_fnma)(A[r][i], xi, b[r]);
@@ -274,6 +256,8 @@ static void SFX(lu_solve)(int N, CX A[][ORC_NMAX], CX* b, CX* z) {
     z[i] = xi;
   }
 }
+
+static void SFX(lu_solve)(int N, CX A[][ORC_NMAX], CX* b, CX* z) { SFX(lu_solve_trace)(N, A, b, z, NULL, NULL); }
 
 /* one evaluation + solve: z = H_x^{-1} * rhs; rhs = -H_t (which=1) or H (which=0) */
 static void SFX(eval_solve)(const orc_problem* pb, const COEFS* cf, const CX* x, int which, CX* z) {
@@ -503,6 +487,22 @@ int SFX(orc_lu_solve)(int32_t N, const REAL* A_rowmajor, const REAL* b, REAL* z)
     bb[r] = SFX(c_make)(b[2 * r], b[2 * r + 1]);
   }
   SFX(lu_solve)(N, A, bb, zz);
+  for (int r = 0; r < N; ++r) {
+    z[2 * r] = zz[r].re;
+    z[2 * r + 1] = zz[r].im;
+  }
+  return 0;
+}
+
+/* One linear solve with its pivot trace (piv [N], mags [N*N], see lu_solve_trace). */
+int SFX(orc_lu_pivots)(int32_t N, const REAL* A_rowmajor, const REAL* b, REAL* z, int32_t* piv, REAL* mags) {
+  if (N < 1 || N > ORC_NMAX) return -1;
+  CX A[ORC_NMAX][ORC_NMAX], bb[ORC_NMAX], zz[ORC_NMAX];
+  for (int r = 0; r < N; ++r) {
+    for (int c = 0; c < N; ++c) A[r][c] = SFX(c_make)(A_rowmajor[2 * (r * N + c)], A_rowmajor[2 * (r * N + c) + 1]);
+    bb[r] = SFX(c_make)(b[2 * r], b[2 * r + 1]);
+  }
+  SFX(lu_solve_trace)(N, A, bb, zz, piv, mags);
   for (int r = 0; r < N; ++r) {
     z[2 * r] = zz[r].re;
     z[2 * r + 1] = zz[r].im;

@@ -385,6 +385,22 @@ def lu_solve(A, b, precision="d"):
     return z[:, 0].astype(np.float64) + 1j * z[:, 1].astype(np.float64)
 
 
+def lu_pivots(A, b, precision="d"):
+    """One linear solve with its pivot trace: (z [N], piv [N] = the pivot position of each column,
+    mags [N, N] = |Re|+|Im| of the row at position j when column i was searched, j >= i)."""
+    rt = np.float64 if precision == "d" else np.float32
+    fn = lib().orc_lu_pivots_d if precision == "d" else lib().orc_lu_pivots_f
+    N = A.shape[0]
+    a, bb = _cx(A, rt), _cx(b, rt)
+    z = np.zeros((N, 2), rt)
+    piv = np.zeros(N, np.int32)
+    mags = np.full((N, N), np.nan, rt)
+    P = ctypes.c_void_p
+    fn.argtypes = [ctypes.c_int32, P, P, P, P, P]
+    assert fn(N, a.ctypes.data, bb.ctypes.data, z.ctypes.data, piv.ctypes.data, mags.ctypes.data) == 0
+    return z[:, 0].astype(np.float64) + 1j * z[:, 1].astype(np.float64), piv, mags
+
+
 # ----------------------------------------------------------------------------
 # result counts (Evaluations.cpp:88-176 restated)
 # ----------------------------------------------------------------------------

@@ -44,31 +44,32 @@ def inputs(name, n_hyp=1, seed=0):
     return pb, ob, np.array(tg)
 
 
-def run_gpu(pb, ob, targets, precision, polish=0, p2c="oracle", **kw):
+def run_gpu(pb, ob, targets, precision, polish=0, p2c="oracle", start=None, **kw):
     n_hyp = len(targets)
+    start = ob.start_params if start is None else start
     rt = torch.float32 if precision == ghc.PREC_FP32 else torch.float64
     ws = ghc.Workspace(pb, n_hyp, precision)
     ss = cx_t(ob.start_sols, rt)
     if pb.kind == ghc.KIND_P2C:
         if p2c == "device":
-            dhx, dht = pb.p2c_device(cx_t(ob.start_params), cx_t(targets))
+            dhx, dht = pb.p2c_device(cx_t(start), cx_t(targets))
             hx, ht = to_cx(dhx), to_cx(dht)[:, : (pb.M + 1) * pb.K]
         else:
-            hx = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[0] for t in targets])
-            ht = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[1] for t in targets])
+            hx = np.array([O.p2c_tables(ob.terms, start, t)[0] for t in targets])
+            ht = np.array([O.p2c_tables(ob.terms, start, t)[1] for t in targets])
             dhx, dht = cx_t(hx), cx_t(ht)
         ghc.track(pb, ws, ss, d_coef_hx=dhx, d_coef_ht=dht, polish_iters=polish, **kw)
         oargs = dict(hx=hx, ht=ht)
     else:
-        ps = cx_t(ob.start_params)
+        ps = cx_t(start)
         pt = cx_t(targets)
         if precision == ghc.PREC_FP32:
             # the FP32 oracle subtracts in float: hand the kernel the same rounded difference
-            pd = cx_t(targets.astype(np.complex64) - ob.start_params.astype(np.complex64)[None, :])
+            pd = cx_t(targets.astype(np.complex64) - start.astype(np.complex64)[None, :])
         else:
-            pd = cx_t(targets - ob.start_params[None, :])
+            pd = cx_t(targets - start[None, :])
         ghc.track(pb, ws, ss, d_p_start=ps, d_p_target=pt, d_p_diff=pd, polish_iters=polish, **kw)
-        oargs = dict(p_start=ob.start_params, p_target=targets)
+        oargs = dict(p_start=start, p_target=targets)
     torch.cuda.synchronize()
     return ws, oargs
 
@@ -226,6 +227,28 @@ def test_mixed_precision_recall(name):
     assert found >= 0.995 * real64.sum(), (found, real64.sum())
     rmx = wmx.resid.cpu().numpy()[cmx]
     assert np.median(rmx) < 1e-10
+
+
+@pytest.mark.parametrize("name,step", [("generalized_3views_4pts", "reference"), ("generalized_3views_4pts", "robust"),
+                                       ("uncalibrated_trifocal_rel_pos_CY", "reference"),
+                                       ("uncalibrated_trifocal_rel_pos_CY", "robust"), ("P3P_TD", "reference"),
+                                       ("trifocal_2op1p_30x30", "reference")])
+def test_scene_targets_bit_exact_vs_oracle(name, step):
+    """The seeded scene generators the benchmarks draw from (scenes.py: generalized 3-view 4-point
+    scenes with 0.5 px noise, uncalibrated trifocal scenes with 30 % outliers, P3P by total degree,
+    trifocal 30x30 from points and tangents): the FP64 tracker equals the oracle bit for bit on
+    those targets, polished endpoints and residuals included, under both step controls."""
+    import scenes
+    pb, ob = ghc.Problem(name), O.Problem(name)
+    st, tg, _ = scenes.targets_for(name, 3, 17, ob.start_params, ob.target_params)
+    kw = ROBUST if step == "robust" else {}
+    okw = dict(step=O.ROBUST_STEP, max_corr=3, max_steps=2000) if step == "robust" else {}
+    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_FP64, polish=3, start=st, **kw)
+    r = O.track(ob, ob.start_sols, polish_iters=3, nthreads=NCPU, **oargs, **okw)
+    compare(ws, r)
+    conv = r["conv"] == 1
+    assert conv.mean() > 0.5
+    assert np.array_equal(ws.resid.cpu().numpy()[conv], r["resid"][conv])
 
 
 def test_step_cap_and_short_corrector():

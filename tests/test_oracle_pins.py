@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from lu_cases import SIZES, cases, strict_argmax
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "cy_golden_tracks.txt")
 P2C_PROBLEMS = ["P3P", "5pt_rel_pos_alg_form_quat", "generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY",
@@ -205,3 +206,29 @@ def test_oracle_two_phase_mixed():
     plain = O.track(pb, pb.start_sols, hx=hx, ht=ht, polish_iters=3, nthreads=4)
     zero = O.track(pb, pb.start_sols, hx=hx, ht=ht, precision="mixed", t_switch=0.0, polish_iters=3, nthreads=4)
     assert np.array_equal(plain["endpoints"], zero["endpoints"])
+
+
+@pytest.mark.parametrize("prec", ["d", "f"])
+def test_lu_pivot_rule_is_reference_scan(prec):
+    """The oracle's pivot of every column is the reference's strict-argmax scan
+    (dev-cgesv-batched-small.cuh:54-65) over the magnitudes it saw: random matrices, exact and
+    near ties (one ulp apart), zero pivots and NaN; on exact ties the lowest position wins."""
+    rt = np.float64 if prec == "d" else np.float32
+    checked = ties = 0
+    for N in SIZES:
+        for kind, A, b in cases(N, rt):
+            _, piv, mags = O.lu_pivots(A, b, prec)
+            for i in range(N):
+                assert piv[i] == strict_argmax(mags[i], i), (kind, N, i)
+                col = mags[i, i:]
+                top = np.nanmax(col) if np.isfinite(col).any() else np.nan
+                ties += int(np.sum(col == top) > 1)
+                checked += 1
+            if kind == "near ties" and np.isfinite(mags[0]).all():
+                # the larger magnitude, one unit in the last place above the others, is taken
+                assert piv[0] == N - 1
+            if kind == "nan first":
+                assert piv[0] == 0
+            if kind == "exact ties":
+                assert piv[0] == int(np.argmax(mags[0] == np.max(mags[0])))
+    assert checked > 1000 and ties > 100

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/ghc.h"
+#include "abi_internal.h"
 #include "ghc_internal.h"
 #include "problem.h"
 
@@ -19,15 +20,6 @@ int launch_f2d(const float* s, double* d, long long n, void* stream);
 int launch_debug_f(const uint8_t* conv, const double* t, const double* dt, float* dbg, long long n, void* stream);
 int launch_debug_d(const uint8_t* conv, const double* t, const double* dt, double* dbg, long long n, void* stream);
 int launch_diff_d(const double* s, const double* t, double* d, long long n_hyp, int P1, void* stream);
-}  // namespace ghc
-
-using namespace ghc;
-
-struct ghc_problem {
-  Problem pb;
-};
-
-namespace {
 
 int sm_count() {
   int dev = 0, n = 0;
@@ -120,6 +112,76 @@ PolishParams polish_params(const TrackParams& t, double* endpoints, const uint8_
   q.iters = iters;
   return q;
 }
+
+int track_params(const Problem& pb, const ghc_track_args* a, TrackParams& p) {
+  p = base_params(pb);
+  apply_tuning(pb, a->precision, p);
+  if (a->max_steps > 0) p.max_steps = a->max_steps;
+  if (a->max_corr > 0) p.max_corr = a->max_corr;
+  if (a->incr_steps > 0) p.incr = a->incr_steps;
+  p.n_items = a->n_hyp * (long long)(a->paths > 0 ? a->paths : pb.paths);
+  p.paths_per_hyp = a->paths > 0 ? a->paths : pb.paths;
+  p.start_sols = a->d_start_sols;
+  p.ld_start = pb.N;
+  p.track_in = nullptr;
+  p.ld_track = pb.N;
+  if (pb.kind == KIND_P2C) {
+    if (!a->d_coef_hx || !a->d_coef_ht) {
+      set_error("P2C problem needs d_coef_hx / d_coef_ht");
+      return GHC_ERR_ARG;
+    }
+    p.coef_hx = a->d_coef_hx;
+    p.coef_ht = a->d_coef_ht;
+    p.stride_hx = (long long)(pb.M + 1) * (pb.K + 1);
+    p.stride_ht = (long long)(pb.M + 1) * pb.K;
+  } else {
+    if (!a->d_p_start || !a->d_p_target || !a->d_p_diff) {
+      set_error("PH problem needs d_p_start / d_p_target / d_p_diff");
+      return GHC_ERR_ARG;
+    }
+    p.p_start = a->d_p_start;
+    p.p_tgt = a->d_p_target;
+    p.p_diff = a->d_p_diff;
+    p.stride_p = pb.P + 1;
+  }
+  p.endpoints = a->d_endpoints;
+  p.ld_out = pb.N;
+  p.status = a->d_status;
+  p.conv = a->d_conv;
+  p.infy = a->d_inf;
+  p.steps = a->d_steps;
+  p.corr = a->d_corr;
+  p.t_end = a->d_t_end;
+  p.dt_end = a->d_dt_end;
+  p.counter = a->d_counter;
+  if (a->corr_tol2 > 0) p.corr_tol2 = a->corr_tol2;
+  if (a->first_tol2 > 0) p.first_tol2 = a->first_tol2;
+  if (a->dt_max > 0) p.dt_max = a->dt_max;
+  if (a->cond_limit > 0) p.cond_limit = a->cond_limit;
+  return GHC_OK;
+}
+
+int run_track(const TrackParams& p, const ghc_track_args* a, void* stream) {
+  int rc = track_code(launch_track(p, a->precision, a->t_switch, stream, sm_count()));
+  if (rc) return rc;
+  const bool fp64_state = a->precision == GHC_PREC_FP64 || a->precision == GHC_PREC_MIXED;
+  if ((a->polish_iters > 0 || a->d_resid) && fp64_state) {
+    if (!a->d_conv) {
+      set_error("polish needs d_conv");
+      return GHC_ERR_ARG;
+    }
+    PolishParams q = polish_params(p, (double*)a->d_endpoints, a->d_conv, a->d_resid, a->polish_iters);
+    rc = launch_polish(q, stream);
+    if (rc) return track_code(rc);
+  }
+  return GHC_OK;
+}
+
+}  // namespace ghc
+
+using namespace ghc;
+
+namespace {
 
 // Pointer array of the reference layout: entry p == base + p * (N+1) complex.
 template <typename T>
@@ -319,6 +381,7 @@ int ghc_problem_get_info(const ghc_problem* h, ghc_problem_info* info) {
   info->n_ht_terms = (int)pb.ht_off.back();
   info->has_p2c_terms = pb.has_terms ? 1 : 0;
   info->subwarp = track_subwarp_width(pb.N);
+  info->device = pb.dev.device;
   return GHC_OK;
 }
 
@@ -419,62 +482,9 @@ int ghc_track(const ghc_problem* h, const ghc_track_args* a, void* stream) {
   Problem& pb = const_cast<Problem&>(h->pb);
   int rc = ensure_device(pb);
   if (rc) return rc;
-  TrackParams p = base_params(pb);
-  apply_tuning(pb, a->precision, p);
-  if (a->max_steps > 0) p.max_steps = a->max_steps;
-  if (a->max_corr > 0) p.max_corr = a->max_corr;
-  if (a->incr_steps > 0) p.incr = a->incr_steps;
-  p.n_items = a->n_hyp * (long long)(a->paths > 0 ? a->paths : pb.paths);
-  p.paths_per_hyp = a->paths > 0 ? a->paths : pb.paths;
-  p.start_sols = a->d_start_sols;
-  p.ld_start = pb.N;
-  p.track_in = nullptr;
-  p.ld_track = pb.N;
-  if (pb.kind == KIND_P2C) {
-    if (!a->d_coef_hx || !a->d_coef_ht) {
-      set_error("P2C problem needs d_coef_hx / d_coef_ht");
-      return GHC_ERR_ARG;
-    }
-    p.coef_hx = a->d_coef_hx;
-    p.coef_ht = a->d_coef_ht;
-    p.stride_hx = (long long)(pb.M + 1) * (pb.K + 1);
-    p.stride_ht = (long long)(pb.M + 1) * pb.K;
-  } else {
-    if (!a->d_p_start || !a->d_p_target || !a->d_p_diff) {
-      set_error("PH problem needs d_p_start / d_p_target / d_p_diff");
-      return GHC_ERR_ARG;
-    }
-    p.p_start = a->d_p_start;
-    p.p_tgt = a->d_p_target;
-    p.p_diff = a->d_p_diff;
-    p.stride_p = pb.P + 1;
-  }
-  p.endpoints = a->d_endpoints;
-  p.ld_out = pb.N;
-  p.status = a->d_status;
-  p.conv = a->d_conv;
-  p.infy = a->d_inf;
-  p.steps = a->d_steps;
-  p.corr = a->d_corr;
-  p.t_end = a->d_t_end;
-  p.dt_end = a->d_dt_end;
-  p.counter = a->d_counter;
-  if (a->corr_tol2 > 0) p.corr_tol2 = a->corr_tol2;
-  if (a->first_tol2 > 0) p.first_tol2 = a->first_tol2;
-  if (a->dt_max > 0) p.dt_max = a->dt_max;
-  rc = track_code(launch_track(p, a->precision, a->t_switch, stream, sm_count()));
-  if (rc) return rc;
-  const bool fp64_state = a->precision == GHC_PREC_FP64 || a->precision == GHC_PREC_MIXED;
-  if ((a->polish_iters > 0 || a->d_resid) && fp64_state) {
-    if (!a->d_conv) {
-      set_error("polish needs d_conv");
-      return GHC_ERR_ARG;
-    }
-    PolishParams q = polish_params(p, (double*)a->d_endpoints, a->d_conv, a->d_resid, a->polish_iters);
-    rc = launch_polish(q, stream);
-    if (rc) return track_code(rc);
-  }
-  return GHC_OK;
+  TrackParams p;
+  if ((rc = track_params(pb, a, p))) return rc;
+  return run_track(p, a, stream);
 }
 
 int ghc_count_results(int32_t N, int32_t paths, const double* z, const uint8_t* conv, const uint8_t* inf,

@@ -183,6 +183,9 @@ struct TrackParams {
   double corr_tol2;   // corrector success: |dx|^2 < corr_tol2 |x|^2
   double first_tol2;  // reject when the first Newton update has |dx|^2 > first_tol2 |x|^2
   double dt_max;      // step-size cap
+  // mixed tracker: stop a path (handover) after a step in which a solve's pivot magnitudes spanned
+  // more than cond_limit, or one was NaN (0: never)
+  double cond_limit;
 };
 
 struct PolishParams {

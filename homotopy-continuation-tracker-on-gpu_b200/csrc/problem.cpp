@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <fstream>
@@ -276,6 +277,8 @@ int load_problem(const std::string& root, const std::string& name, Problem& pb) 
     set_error("cannot read " + dir + "/gpuhc_settings.yaml");
     return GHC_ERR_IO;
   }
+  static std::atomic<uint64_t> next_uid{1};
+  pb.uid = next_uid++;
   pb.name = name;
   pb.print_name = kv.count("problem_print_out_name") ? kv["problem_print_out_name"] : name;
   pb.type = kv.count("GPUHC_Type") ? kv["GPUHC_Type"] : "";

@@ -59,6 +59,7 @@ struct Problem {
   int tune_variant[2] = {0, 0};
   int tune_flat[2] = {-1, -1};
   DeviceTables dev;
+  uint64_t uid = 0;  // unique per loaded handle (set by load_problem; never reused in a process)
   ~Problem();
 };
 

@@ -5,15 +5,20 @@
 // sizes cover every problem of the reference (P2C with N in
 // {3,4,5,6,8,10,11,12,16,18}, PH with N = 30); others are rejected.
 //
-// Mixed precision is two launches on one stream.  The FP32 tracker takes every
-// path from t = 0 to t_switch; a path that fails kMixedFailLimit steps in a row
-// or diverges is handed over early, always at its last accepted point.  It
-// writes its float track into the first half of each item's double endpoint
-// slot and t, dt, step and corrector counts into t_end, dt_end, steps, corr.
-// The FP64 tracker then resumes every path from there (reading the float track
-// in place) to t = 1, so the end game, every retried stretch and the final
-// answer are FP64.  The FP32 phase asks its corrector for no more than float
-// can deliver: |dx|^2 < max(corr_tol2, kMixedF32Tol2) |x|^2.
+// Mixed precision is two launches on one stream.  The mixed tracker keeps the
+// track, t, the step control, the norms and the corrector's residual H in FP64
+// and evaluates H_x and H_t and factors the system in FP32 (Newton with an FP32
+// solve of an FP64 residual: the endpoints converge to FP64 accuracy at a rate
+// set by the FP32 solve, about cond(H_x) times FP32's rounding).  It takes every
+// path to t = 1 (or to t_switch, when t_switch < 1); a path stops early after a
+// step in which an FP32 solve's pivot magnitudes spanned more than cond_limit
+// (the Jacobian is too ill-conditioned for FP32: Newton would stall), after
+// kMixedFailLimit failed steps in a row, or on divergence (then at its last
+// accepted point), with t, dt and its step and corrector counts in t_end,
+// dt_end, steps and corr.  The FP64 tracker then resumes every
+// path from there: a path the mixed tracker finished stops at once, a handed-over
+// one continues with FP64 linear algebra (ill-conditioned Jacobians near a
+// singular endpoint).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,38 +35,36 @@ int track_subwarp_width(int N) {
   return 32;
 }
 
-constexpr int kMixedFailLimit = 2;
-constexpr double kMixedMaxSwitch = 0.95;
-constexpr double kMixedF32Tol2 = 1e-9;
+constexpr int kMixedFailLimit = 4;
+constexpr double kMixedCondLimit = 1e4;
 
 int launch_track(const TrackParams& p, int precision, double t_switch, void* stream, int n_sm) {
   cudaStream_t s = (cudaStream_t)stream;
   if (p.n_items <= 0) return 0;
+  TrackParams q = p;
+  q.cond_limit = 0.0;  // the plain trackers never stop on conditioning
   switch (precision) {
     case PREC_FP64:
-      return launch_track_fp64(p, s, n_sm);
+      return launch_track_fp64(q, s, n_sm);
     case PREC_FP32:
-      return launch_track_fp32(p, s, n_sm);
+      return launch_track_fp32(q, s, n_sm);
     case PREC_MIXED: {
       if (!p.t_end || !p.dt_end || !p.steps || !p.corr || p.track_in || p.resume) return -12;
-      if (!(t_switch > 0.0)) return launch_track_fp64(p, s, n_sm);
+      if (!(t_switch > 0.0)) return launch_track_fp64(q, s, n_sm);
       TrackParams a = p;
-      a.t_handover = std::min(t_switch, kMixedMaxSwitch);
+      a.t_handover = t_switch < 1.0 ? t_switch : 0.0;  // 0: no time boundary, the whole path
       a.fail_limit = kMixedFailLimit;
+      a.cond_limit = p.cond_limit > 0.0 ? p.cond_limit : kMixedCondLimit;
       a.variant = p.variant_f32;
       a.flat_eval = p.flat_eval_f32;
-      a.corr_tol2 = std::max(p.corr_tol2, kMixedF32Tol2);
-      a.start_other = 1;        // double start solutions into the FP32 tracker
-      a.ld_out = 2 * p.ld_out;  // float track in the first half of each double slot
-      int rc = launch_track_fp32(a, s, n_sm);
+      int rc = launch_track_mixed(a, s, n_sm);
       if (rc) return rc;
-      TrackParams b = p;
+      TrackParams b = q;
       b.resume = 1;
       b.t_in = p.t_end;
       b.dt_in = p.dt_end;
       b.track_in = p.endpoints;
-      b.ld_track = 2 * p.ld_out;
-      b.track_other = 1;
+      b.ld_track = p.ld_out;
       return launch_track_fp64(b, s, n_sm);
     }
     default:

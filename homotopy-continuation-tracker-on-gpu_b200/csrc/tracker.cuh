@@ -134,41 +134,47 @@ __device__ __forceinline__ cx<R> acc_term(cx<R> acc, cx<R> p, uint64_t w, const 
   }
 }
 
-// c_k(t), c'_k(t) for k = l, l+W, ... (reference eval_parameter_homotopy)
-template <typename R, int W>
+// c_k(t), c'_k(t) for k = l, l+W, ... (reference eval_parameter_homotopy), computed in R and
+// stored in RO; with HI the R values of c_k(t) are also kept in hi (the residual's copy)
+template <typename R, typename RO, int W, bool HI>
 __device__ __forceinline__ void coef_eval_p2c(const double* __restrict__ hx, const double* __restrict__ ht, int M,
-                                              int K, R t, cx<R>* c, cx<R>* cp, int l) {
+                                              int K, R t, cx<RO>* c, cx<RO>* cp, cx<R>* hi, int l) {
   for (int k = l; k <= M; k += W) {
     const double* a = hx + 2 * (size_t)k * (K + 1);
     cx<R> v = mk((R)__ldg(a + 2 * K), (R)__ldg(a + 2 * K + 1));
     for (int j = K - 1; j >= 0; --j) v = mk(f_fma(v.re, t, (R)__ldg(a + 2 * j)), f_fma(v.im, t, (R)__ldg(a + 2 * j + 1)));
-    c[k] = v;
+    c[k] = c_cast<RO>(v);
+    if (HI) hi[k] = v;
     if (K >= 1) {
       const double* b = ht + 2 * (size_t)k * K;
       cx<R> u = mk((R)__ldg(b + 2 * (K - 1)), (R)__ldg(b + 2 * (K - 1) + 1));
       for (int j = K - 2; j >= 0; --j) u = mk(f_fma(u.re, t, (R)__ldg(b + 2 * j)), f_fma(u.im, t, (R)__ldg(b + 2 * j + 1)));
-      cp[k] = u;
+      cp[k] = c_cast<RO>(u);
     } else {
-      cp[k] = mk(R(0), R(0));
+      cp[k] = mk(RO(0), RO(0));
     }
   }
 }
 
-// p(t) = p1 t + p0 (1-t) and the parameter differences (reference compute_param_homotopy)
-template <typename R, int W>
+// p(t) = p1 t + p0 (1-t) and the parameter differences (reference compute_param_homotopy), computed
+// in R and stored in RO; with HI the R values of p(t) are also kept in hi
+template <typename R, typename RO, int W, bool HI>
 __device__ __forceinline__ void coef_eval_ph(const double* __restrict__ ps, const double* __restrict__ pt,
-                                             const double* __restrict__ pd, int P, R t, cx<R>* ph, cx<R>* dp,
-                                             int l) {
+                                             const double* __restrict__ pd, int P, R t, cx<RO>* ph, cx<RO>* dp,
+                                             cx<R>* hi, int l) {
   const R u = f_sub(R(1), t);
   for (int k = l; k < P; k += W) {
     const R gr = (R)__ldg(pt + 2 * k), gi = (R)__ldg(pt + 2 * k + 1);
     const R sr = (R)__ldg(ps + 2 * k), si = (R)__ldg(ps + 2 * k + 1);
-    ph[k] = mk(f_fma(gr, t, f_mul(sr, u)), f_fma(gi, t, f_mul(si, u)));
-    dp[k] = mk((R)__ldg(pd + 2 * k), (R)__ldg(pd + 2 * k + 1));
+    const cx<R> v = mk(f_fma(gr, t, f_mul(sr, u)), f_fma(gi, t, f_mul(si, u)));
+    ph[k] = c_cast<RO>(v);
+    if (HI) hi[k] = v;
+    dp[k] = mk((RO)__ldg(pd + 2 * k), (RO)__ldg(pd + 2 * k + 1));
   }
   if (l == 0) {
-    ph[P] = mk(R(1), R(0));
-    dp[P] = mk((R)__ldg(pd + 2 * P), (R)__ldg(pd + 2 * P + 1));
+    ph[P] = mk(RO(1), RO(0));
+    if (HI) hi[P] = mk(R(1), R(0));
+    dp[P] = mk((RO)__ldg(pd + 2 * P), (RO)__ldg(pd + 2 * P + 1));
   }
 }
 
@@ -180,7 +186,7 @@ __device__ __forceinline__ cx<R> term_coef_value(uint64_t w, const cx<R>* ca) {
   return c_mul(p, ca[term_pb(w)]);
 }
 
-// Row r of H_x into A, and b = H (which = 0) or -H_t (which = 1).
+// Row r of H_x into A.
 //
 // Flat (always above 16 unknowns, else when the problem's flat_eval is set):
 // the row's terms are walked as one list (CSR row r, entry ends flagged in the term word),
@@ -199,10 +205,35 @@ __device__ __forceinline__ cx<R> term_coef_value(uint64_t w, const cx<R>* ca) {
 template <int N>
 constexpr bool kFlatAlways = N > 16;
 
-template <typename R, int N, int W, int KIND, int NVX, int NVT>
-__device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, const cx<R>* cb, const cx<R>* xs, int r,
-                                         bool live, cx<R> (&A)[N], cx<R>& b, int which, int walk,
-                                         unsigned char* scr, unsigned nz) {
+// Row r of H (which = 0) or of -H_t (which = 1) from the H_t term table, in precision R
+template <typename R, int N, int KIND, int NVT>
+__device__ __forceinline__ cx<R> eval_rhs(const Tables& tb, const cx<R>* ca, const cx<R>* cb, const cx<R>* xs, int r,
+                                          bool live, int which) {
+  cx<R> h = mk(R(0), R(0));
+  if (live) {
+    const int len = tb.ht_off[r + 1] - tb.ht_off[r];
+    for (int k = 0; k < len; ++k) {
+      const uint64_t w = tb.ht_terms[k * N + r];
+      cx<R> p;
+      if (KIND == KIND_P2C) {
+        p = c_scale((R)term_scale(w), which ? cb[term_coef(w)] : ca[term_coef(w)]);
+      } else if (which) {
+        const int a = term_pa(w), bb = term_pb(w);
+        const cx<R> u = c_fma(cb[bb], ca[a], c_mul(cb[a], ca[bb]));
+        p = c_scale((R)term_scale(w), u);
+      } else {
+        p = c_scale((R)term_scale(w), ca[term_pa(w)]);
+        p = c_mul(p, ca[term_pb(w)]);
+      }
+      h = acc_term<R, NVT>(h, p, w, xs);
+    }
+  }
+  return which ? mk(-h.re, -h.im) : h;
+}
+
+template <typename R, int N, int W, int KIND, int NVX>
+__device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, const cx<R>* xs, int r, bool live,
+                                         cx<R> (&A)[N], int walk, unsigned char* scr, unsigned nz) {
   auto slot = [&](int k) -> cx<R>* { return view<R>(scr) + (k * W + r); };
   const int lanes = balanced_walk_built(N) ? tb.hx_off[N * N + 1] : kNoLanes;
   const bool balanced = balanced_walk_built(N) && walk == 2 && lanes != kNoLanes;
@@ -256,32 +287,12 @@ __device__ __forceinline__ void eval_row(const Tables& tb, const cx<R>* ca, cons
     for (int i = 0; i < N; ++i)
       A[i] = ((nz >> i) & 1u) ? *slot(__popc(nz & ((1u << i) - 1u))) : mk(R(0), R(0));
   }
-  cx<R> h = mk(R(0), R(0));
-  if (live) {
-    const int len = tb.ht_off[r + 1] - tb.ht_off[r];
-    for (int k = 0; k < len; ++k) {
-      const uint64_t w = tb.ht_terms[k * N + r];
-      cx<R> p;
-      if (KIND == KIND_P2C) {
-        p = c_scale((R)term_scale(w), which ? cb[term_coef(w)] : ca[term_coef(w)]);
-      } else if (which) {
-        const int a = term_pa(w), bb = term_pb(w);
-        const cx<R> u = c_fma(cb[bb], ca[a], c_mul(cb[a], ca[bb]));
-        p = c_scale((R)term_scale(w), u);
-      } else {
-        p = c_scale((R)term_scale(w), ca[term_pa(w)]);
-        p = c_mul(p, ca[term_pb(w)]);
-      }
-      h = acc_term<R, NVT>(h, p, w, xs);
-    }
-  }
-  b = which ? mk(-h.re, -h.im) : h;
 }
 
 // Pivot key of a row for column i: magnitude |Re|+|Im| cut to its upper bits, position in the
 // low 5 bits (largest key = largest cut magnitude, lowest position among equal ones).  Pivoted
 // rows 0; a NaN at the current position wins, a NaN below never does.  The cut only speeds up the
-// search: pivot_search resolves every near tie on the full magnitudes.
+// search: a near tie it gets wrong is found and redone on the full magnitudes (pivot_exact).
 __device__ __forceinline__ unsigned mag_bits(double v) { return (unsigned)__double2hiint(v); }
 __device__ __forceinline__ unsigned mag_bits(float v) { return __float_as_uint(v); }
 template <typename R>
@@ -323,73 +334,108 @@ constexpr int LU_UNROLLED = 0, LU_ROLLED = 1;
 template <int N>
 constexpr int kLuForm = N <= 16 ? LU_UNROLLED : GHC_LU_LARGE;
 
-// Pivot position of column i, the reference's rule (dev-cgesv-batched-small.cuh:54-65): the
-// largest |Re|+|Im| among the unpivoted rows, the lowest position among equal magnitudes, a NaN
-// at position i kept and a NaN below never taken.  An integer max butterfly over pivot_key finds
-// it in one shuffle per level; that answer is exact unless another unpivoted row shares the
-// winner's cut magnitude, and then (in any sub-warp of the warp) the full magnitudes and the
-// positions are reduced as pairs.
+// Pivot position of column i by the reference's rule (dev-cgesv-batched-small.cuh:54-65): the
+// largest |Re|+|Im| among the unpivoted rows, the lowest position among equal magnitudes, a NaN at
+// position i kept and a NaN below never taken.  Two steps:
+//   pivot_fast   an integer max butterfly over pivot_key (one shuffle per level): the largest cut
+//                magnitude, the lowest position among equal cut magnitudes;
+//   cut_was_wrong  after the chosen row is broadcast, true on a lane whose row shares the winner's
+//                cut magnitude but has a strictly larger full one -- the only way the cut choice
+//                can differ from the exact one (equal full magnitudes are ordered by position in
+//                both);
+//   pivot_exact  the full magnitudes and the positions reduced as pairs, run (by the whole warp)
+//                only when some lane saw cut_was_wrong.
 template <typename R, int W>
-__device__ __forceinline__ int pivot_search(cx<R> a, bool live, int pos, int i) {
-  const R m = fabs(a.re) + fabs(a.im);
-  const unsigned key = live ? pivot_key(m, pos, i) : 0u;
+__device__ __forceinline__ unsigned pivot_fast(unsigned key) {
   unsigned best = key;
 #pragma unroll
   for (int off = W / 2; off > 0; off >>= 1) best = max(best, __shfl_xor_sync(kFull, best, off, W));
-  const bool cand = live && pos >= i;
-  const unsigned near = __ballot_sync(kFull, cand && ((key ^ best) >> 5) == 0u);
-  const unsigned mine = (W == 32) ? near : (near >> ((threadIdx.x & 31) & ~(W - 1))) & ((1u << (W & 31)) - 1u);
-  if (__any_sync(kFull, __popc(mine) > 1)) {
-    // (magnitude bits, position): non-negative magnitudes order as their bit patterns; a NaN at
-    // position i first, a NaN below and the pivoted rows last
-    unsigned long long mb = 0ull;
-    int mp = 64;
-    if (cand) {
-      if (m == m) {
-        mb = full_bits(m);
-        mp = pos;
-      } else if (pos == i) {
-        mb = ~0ull;
-        mp = pos;
-      }
+  return best;
+}
+template <typename R>
+__device__ __forceinline__ bool cut_was_wrong(R m, unsigned key, unsigned best, bool cand, R pm) {
+  return cand && ((key ^ best) >> 5) == 0u && m > pm;
+}
+template <typename R, int W>
+__device__ __forceinline__ int pivot_exact(R m, bool cand, int pos, int i) {
+  // (magnitude bits, position): non-negative magnitudes order as their bit patterns; a NaN at
+  // position i first, a NaN below and the pivoted rows last
+  unsigned long long mb = 0ull;
+  int mp = 64;
+  if (cand) {
+    if (m == m) {
+      mb = full_bits(m);
+      mp = pos;
+    } else if (pos == i) {
+      mb = ~0ull;
+      mp = pos;
     }
-#pragma unroll
-    for (int off = W / 2; off > 0; off >>= 1) {
-      const unsigned long long ob = __shfl_xor_sync(kFull, mb, off, W);
-      const int op = __shfl_xor_sync(kFull, mp, off, W);
-      if (ob > mb || (ob == mb && op < mp)) {
-        mb = ob;
-        mp = op;
-      }
-    }
-    return mp;
   }
-  return 31 - (int)(best & 31u);
+#pragma unroll
+  for (int off = W / 2; off > 0; off >>= 1) {
+    const unsigned long long ob = __shfl_xor_sync(kFull, mb, off, W);
+    const int op = __shfl_xor_sync(kFull, mp, off, W);
+    if (ob > mb || (ob == mb && op < mp)) {
+      mb = ob;
+      mp = op;
+    }
+  }
+  return mp;
 }
 
-#ifndef GHC_LU_SELECT
-#define GHC_LU_SELECT 0
-#endif
+// PivotRange: the span of the pivot magnitudes |U_ii| (|Re|+|Im|) of one solve and whether one was
+// NaN, the mixed tracker's conditioning test (computed by every solve; unused results cost nothing)
+template <typename R>
+struct PivotRange {
+  R lo, hi;
+  bool nan;
+};
+
 template <typename R, int N, int W>
-__device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
+__device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
+                                                  PivotRange<R>& rg) {
   const bool live = l < N;
   int pos = l;
   static_for<0, N>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     cx<R>* px = sx + (i & 1) * (N + 1);
-    const int bp = pivot_search<R, W>(A[i], live, pos, i);
+    const R m = fabs(A[i].re) + fabs(A[i].im);
+    const bool cand = live && pos >= i;
+    const unsigned key = live ? pivot_key(m, pos, i) : 0u;
+    const unsigned best = pivot_fast<R, W>(key);
+    int bp = 31 - (int)(best & 31u);
+    if (live && pos == bp) {
+      static_for<i, N>([&](auto jc) { px[decltype(jc)::value] = A[decltype(jc)::value]; });
+      px[N] = b;
+    }
+    __syncwarp(kFull);
+    cx<R> p_i = px[i];
+    R pm = fabs(p_i.re) + fabs(p_i.im);
+    if (__any_sync(kFull, cut_was_wrong(m, key, best, cand, pm))) {
+      bp = pivot_exact<R, W>(m, cand, pos, i);
+      __syncwarp(kFull);  // every lane has read the first choice
+      if (live && pos == bp) {
+        static_for<i, N>([&](auto jc) { px[decltype(jc)::value] = A[decltype(jc)::value]; });
+        px[N] = b;
+      }
+      __syncwarp(kFull);
+      p_i = px[i];
+      pm = fabs(p_i.re) + fabs(p_i.im);
+    }
     const bool is_piv = live && (pos == bp);
     if (live) {
       if (pos == bp) pos = i;
       else if (pos == i) pos = bp;
     }
-    if (is_piv) {
-      static_for<i, N>([&](auto jc) { px[decltype(jc)::value] = A[decltype(jc)::value]; });
-      px[N] = b;
+    const bool zero = (pm == R(0));
+    if (i == 0) {
+      rg.lo = rg.hi = pm;
+      rg.nan = pm != pm;
+    } else {
+      rg.lo = fmin(rg.lo, pm);
+      rg.hi = fmax(rg.hi, pm);
+      rg.nan = rg.nan || pm != pm;
     }
-    __syncwarp(kFull);
-    const cx<R> p_i = px[i];
-    const bool zero = (fabs(p_i.re) + fabs(p_i.im) == R(0));
     // (a zero pivot's reciprocal is NaN, as the oracle's c_rcp(0))
     const cx<R> rc = c_rcp(p_i);
     // the pivot row's reciprocal waits in the solution slot of its position until the back
@@ -397,18 +443,6 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
     if (is_piv) sol[i] = rc;
     // rows below the pivot take the update, the others keep their values
     const bool upd = live && pos > i && !zero;
-#if GHC_LU_SELECT
-    // by selects: no branch, so the next column's pivot search can overlap these updates
-    const cx<R> m = c_mul(A[i], rc);
-    A[i] = upd ? m : A[i];
-    static_for<i + 1, N>([&](auto jc) {
-      constexpr int j = decltype(jc)::value;
-      const cx<R> v = c_fnma(m, px[j], A[j]);
-      A[j] = upd ? v : A[j];
-    });
-    const cx<R> vb = c_fnma(m, px[N], b);
-    b = upd ? vb : b;
-#else
     if (upd) {
       A[i] = c_mul(A[i], rc);
       static_for<i + 1, N>([&](auto jc) {
@@ -417,7 +451,6 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
       });
       b = c_fnma(A[i], px[N], b);
     }
-#endif
   });
   static_for<0, N>([&](auto ic) {
     constexpr int i = N - 1 - decltype(ic)::value;
@@ -439,28 +472,50 @@ __device__ __forceinline__ cx<R> pick(const cx<R> (&A)[N], int i) {
 }
 
 template <typename R, int N, int W>
-__device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
+__device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
+                                                PivotRange<R>& rg) {
   const bool live = l < N;
   int pos = l;
   cx<R> myrcp = mk(R(0), R(0));
 #pragma unroll 1
   for (int i = 0; i < N; ++i) {
     cx<R> ai = pick(A, i);
-    const int bp = pivot_search<R, W>(ai, live, pos, i);
-    const bool is_piv = live && (pos == bp);
-    if (live) {
-      if (pos == bp) pos = i;
-      else if (pos == i) pos = bp;
-    }
-    if (is_piv) {
+    const R m = fabs(ai.re) + fabs(ai.im);
+    const bool cand = live && pos >= i;
+    const unsigned key = live ? pivot_key(m, pos, i) : 0u;
+    const unsigned best = pivot_fast<R, W>(key);
+    int bp = 31 - (int)(best & 31u);
+    if (live && pos == bp) {
 #pragma unroll
       for (int j = 0; j < N; ++j)
         if (j >= i) sx[j] = A[j];
       sx[N] = b;
     }
     __syncwarp(kFull);
-    const cx<R> p_i = sx[i];
-    const bool zero = (fabs(p_i.re) + fabs(p_i.im) == R(0));
+    cx<R> p_i = sx[i];
+    R pm = fabs(p_i.re) + fabs(p_i.im);
+    if (__any_sync(kFull, cut_was_wrong(m, key, best, cand, pm))) {
+      bp = pivot_exact<R, W>(m, cand, pos, i);
+      __syncwarp(kFull);  // every lane has read the first choice
+      if (live && pos == bp) {
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+          if (j >= i) sx[j] = A[j];
+        sx[N] = b;
+      }
+      __syncwarp(kFull);
+      p_i = sx[i];
+      pm = fabs(p_i.re) + fabs(p_i.im);
+    }
+    const bool is_piv = live && (pos == bp);
+    if (live) {
+      if (pos == bp) pos = i;
+      else if (pos == i) pos = bp;
+    }
+    const bool zero = (pm == R(0));
+    rg.lo = i == 0 ? pm : fmin(rg.lo, pm);
+    rg.hi = i == 0 ? pm : fmax(rg.hi, pm);
+    rg.nan = (i != 0 && rg.nan) || pm != pm;
     const cx<R> rc = c_rcp(zero ? mk(R(0), R(0)) : p_i);
     if (is_piv) myrcp = rc;
     if (live && pos > i && !zero) {
@@ -485,9 +540,14 @@ __device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, c
 }
 
 template <typename R, int N, int W>
+__device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol, PivotRange<R>& rg) {
+  if constexpr (kLuForm<N> == LU_ROLLED) lu_solve_rolled<R, N, W>(A, b, l, sx, sol, rg);
+  else lu_solve_unrolled<R, N, W>(A, b, l, sx, sol, rg);
+}
+template <typename R, int N, int W>
 __device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
-  if constexpr (kLuForm<N> == LU_ROLLED) lu_solve_rolled<R, N, W>(A, b, l, sx, sol);
-  else lu_solve_unrolled<R, N, W>(A, b, l, sx, sol);
+  PivotRange<R> rg;
+  lu_solve<R, N, W>(A, b, l, sx, sol, rg);
 }
 
 // xor-butterfly sum over the first NP lanes of the sub-warp (order = oracle tree_sum)
@@ -507,9 +567,12 @@ struct SubMem {
   unsigned char* xs;     // track [N+1]
   unsigned char* sx;     // two pivot rows + rhs [2][N+1]
   unsigned char* sol;    // solution [N]
-  unsigned char* state;  // per lane: RK base point x0 [W], RK accumulator [W]
+  unsigned char* state;  // per lane: RK base point x0 [W], RK accumulator [W] (state precision)
   unsigned char* scr;    // H_x row scratch [slots][W], null unless the evaluation is flat
   unsigned char* rec;    // the path's scalar state while the sub-warp evaluates and solves [kRecBytes]
+  unsigned char* coefH;  // mixed: c_k(t) or p(t) in state precision, for the residual H [Mc] (else null)
+  unsigned char* xsH;    // mixed: the track in state precision [N+1] (else null)
+  unsigned char* xst;    // the track in state precision: xsH when mixed, else xs
   unsigned nz;           // this lane's row: bit i set when H_x entry (row, i) has terms
   int walk;              // H_x walk: 0 entry-wise, 1 row-wise, 2 balanced
 };
@@ -525,40 +588,71 @@ __device__ __forceinline__ unsigned row_mask(const uint16_t* hx_off, int r) {
   return m;
 }
 
-// row l of H_x and the right-hand side, term walk of table shape S (EvalShape)
-template <typename R, int N, int W, int KIND, int S>
-__device__ __forceinline__ void eval_any(const Tables& tb, const SubMem& sm, int l, cx<R> (&A)[N], cx<R>& b,
+// Row l of H_x and the right-hand side (which = 1: -H_t, which = 0: H), term walk of table shape S
+// (EvalShape), in the linear-algebra precision RL.  With a state precision R above RL (mixed), the
+// corrector's H is evaluated in R from the R copies of the coefficients and the track, then rounded
+// to RL for the solve: Newton then converges to the R-accurate root at a rate set by the RL solve.
+template <typename R, typename RL, int N, int W, int KIND, int S>
+__device__ __forceinline__ void eval_any(const Tables& tb, const SubMem& sm, int l, cx<RL> (&A)[N], cx<RL>& b,
                                          int which) {
-  eval_row<R, N, W, KIND, shape_nvx(S), shape_nvt(S)>(tb, view<R>(sm.coefA), view<R>(sm.coefB), view<R>(sm.xs), l,
-                                                      l < N, A, b, which, sm.walk, sm.scr, sm.nz);
-}
-
-// one evaluation + solve in precision R; returns this lane's solution component
-template <typename R, int N, int W, int KIND, int S>
-__device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, int l, int which) {
-  cx<R> A[N];
-  cx<R> b;
-  eval_any<R, N, W, KIND, S>(tb, sm, l, A, b, which);
-  lu_solve<R, N, W>(A, b, l, view<R>(sm.sx), view<R>(sm.sol));
-  const cx<R> k = (l < N) ? view<R>(sm.sol)[l] : mk(R(0), R(0));
-  return k;
-}
-
-template <typename R, int N>
-__device__ __forceinline__ void write_track(const SubMem& sm, int l, cx<R> x) {
-  cx<R>* xs = view<R>(sm.xs);
-  if (l < N) xs[l] = x;
-  if (l == 0) xs[N] = mk(R(1), R(0));
-}
-
-template <typename R, int W, int KIND>
-__device__ __forceinline__ void coef_eval(const TrackParams& p, const SubMem& sm, long long hyp, R t, int l) {
-  if (KIND == KIND_P2C) {
-    coef_eval_p2c<R, W>(p.coef_hx + 2 * hyp * p.stride_hx, p.coef_ht + 2 * hyp * p.stride_ht, p.M, p.K, t,
-                        view<R>(sm.coefA), view<R>(sm.coefB), l);
+  eval_row<RL, N, W, KIND, shape_nvx(S)>(tb, view<RL>(sm.coefA), view<RL>(sm.xs), l, l < N, A, sm.walk, sm.scr,
+                                         sm.nz);
+  if constexpr (std::is_same<R, RL>::value) {
+    b = eval_rhs<RL, N, KIND, shape_nvt(S)>(tb, view<RL>(sm.coefA), view<RL>(sm.coefB), view<RL>(sm.xs), l, l < N,
+                                            which);
   } else {
-    coef_eval_ph<R, W>(p.p_start, p.p_tgt + 2 * hyp * p.stride_p, p.p_diff + 2 * hyp * p.stride_p, p.P, t,
-                       view<R>(sm.coefA), view<R>(sm.coefB), l);
+    if (which)
+      b = eval_rhs<RL, N, KIND, shape_nvt(S)>(tb, view<RL>(sm.coefA), view<RL>(sm.coefB), view<RL>(sm.xs), l,
+                                              l < N, 1);
+    else
+      b = c_cast<RL>(eval_rhs<R, N, KIND, shape_nvt(S)>(tb, view<R>(sm.coefH), view<R>(sm.coefH), view<R>(sm.xsH),
+                                                        l, l < N, 0));
+  }
+}
+
+// one evaluation + solve in precision RL; returns this lane's solution component in R.  ill (mixed
+// tracker, cond_limit > 0): the pivot magnitudes spanned more than cond_limit or one was NaN -- the
+// RL solve is too ill-conditioned to keep Newton's contraction
+template <typename R, typename RL, int N, int W, int KIND, int S>
+__device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, int l, int which, double cond_limit,
+                                            bool& ill) {
+  cx<RL> A[N];
+  cx<RL> b;
+  eval_any<R, RL, N, W, KIND, S>(tb, sm, l, A, b, which);
+  PivotRange<RL> rg;
+  lu_solve<RL, N, W>(A, b, l, view<RL>(sm.sx), view<RL>(sm.sol), rg);
+  ill = cond_limit > 0.0 && (rg.nan || !(rg.hi <= (RL)cond_limit * rg.lo));
+  const cx<RL> k = (l < N) ? view<RL>(sm.sol)[l] : mk(RL(0), RL(0));
+  return c_cast<R>(k);
+}
+template <typename R, typename RL, int N, int W, int KIND, int S>
+__device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, int l, int which) {
+  bool ill;
+  return eval_solve<R, RL, N, W, KIND, S>(tb, sm, l, which, 0.0, ill);
+}
+
+// the track into shared memory: in RL for H_x and H_t, and (mixed) in R for the residual
+template <typename R, typename RL, int N>
+__device__ __forceinline__ void write_track(const SubMem& sm, int l, cx<R> x) {
+  cx<RL>* xs = view<RL>(sm.xs);
+  if (l < N) xs[l] = c_cast<RL>(x);
+  if (l == 0) xs[N] = mk(RL(1), RL(0));
+  if constexpr (!std::is_same<R, RL>::value) {
+    cx<R>* xh = view<R>(sm.xsH);
+    if (l < N) xh[l] = x;
+    if (l == 0) xh[N] = mk(R(1), R(0));
+  }
+}
+
+template <typename R, typename RL, int W, int KIND>
+__device__ __forceinline__ void coef_eval(const TrackParams& p, const SubMem& sm, long long hyp, R t, int l) {
+  constexpr bool HI = !std::is_same<R, RL>::value;
+  if (KIND == KIND_P2C) {
+    coef_eval_p2c<R, RL, W, HI>(p.coef_hx + 2 * hyp * p.stride_hx, p.coef_ht + 2 * hyp * p.stride_ht, p.M, p.K, t,
+                                view<RL>(sm.coefA), view<RL>(sm.coefB), view<R>(sm.coefH), l);
+  } else {
+    coef_eval_ph<R, RL, W, HI>(p.p_start, p.p_tgt + 2 * hyp * p.stride_p, p.p_diff + 2 * hyp * p.stride_p, p.P, t,
+                               view<RL>(sm.coefA), view<RL>(sm.coefB), view<R>(sm.coefH), l);
   }
 }
 
@@ -567,25 +661,62 @@ __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t
 __host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
   return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(hx_off_len(N) + N + 1));
 }
-// per sub-warp: the path record [kRecBytes], then in complex values of esz bytes: coefficient
-// buffers [2 Mc], track [N+1], two pivot rows [2 (N+1)], solution [N], lane state [2 W], scratch
-// slots [slots W] (flat)
-__host__ __device__ inline size_t sub_bytes(int N, int Mc, int W, int slots, int esz) {
-  return align16((size_t)esz * (2 * (size_t)Mc + 3 * (N + 1) + N + 2 * W + (size_t)slots * W)) + kRecBytes;
+// Per sub-warp: the path record [kRecBytes], then, in complex values of e bytes (linear-algebra
+// precision): coefficient buffers [2 Mc], track [N+1], two pivot rows [2 (N+1)], solution [N]; the
+// lane state [2 W] in complex values of es bytes (state precision); scratch slots [slots W] (flat);
+// and, when es != e (mixed), the state-precision coefficients [Mc] and track [N+1].
+struct SubOffsets {
+  size_t coefA, coefB, xs, sx, sol, state, scr, coefH, xsH, bytes;
+};
+__host__ __device__ inline SubOffsets sub_offsets(int N, int Mc, int W, int slots, int e, int es) {
+  const bool mixed = es != e;
+  SubOffsets o;
+  size_t off = kRecBytes;
+  o.coefA = off;
+  off += (size_t)e * Mc;
+  o.coefB = off;
+  off += (size_t)e * Mc;
+  o.xs = off;
+  off += (size_t)e * (N + 1);
+  o.sx = off;
+  off += (size_t)e * 2 * (N + 1);
+  o.sol = off;
+  off += (size_t)e * N;
+  if (mixed) off = align16(off);
+  o.state = off;
+  off += (size_t)es * 2 * W;
+  o.scr = off;
+  off += (size_t)e * slots * W;
+  o.coefH = o.xsH = 0;
+  if (mixed) {
+    off = align16(off);
+    o.coefH = off;
+    off += (size_t)es * Mc;
+    o.xsH = off;
+    off += (size_t)es * (N + 1);
+  }
+  o.bytes = kRecBytes + align16(off - kRecBytes);
+  return o;
 }
-template <typename R>
-__device__ __forceinline__ SubMem sub_layout(unsigned char* base, int N, int Mc, int W, bool flat) {
-  constexpr int e = sizeof(cx<R>);
+__host__ __device__ inline size_t sub_bytes(int N, int Mc, int W, int slots, int e, int es) {
+  return sub_offsets(N, Mc, W, slots, e, es).bytes;
+}
+template <typename R, typename RL>
+__device__ __forceinline__ SubMem sub_layout(unsigned char* base, int N, int Mc, int W, int slots, bool flat) {
+  const SubOffsets o = sub_offsets(N, Mc, W, flat ? slots : 0, (int)sizeof(cx<RL>), (int)sizeof(cx<R>));
   SubMem sm;
   sm.rec = base;
-  base += kRecBytes;
-  sm.coefA = base;
-  sm.coefB = base + e * (size_t)Mc;
-  sm.xs = base + 2 * e * (size_t)Mc;
-  sm.sx = sm.xs + e * (N + 1);
-  sm.sol = sm.sx + 2 * e * (N + 1);
-  sm.state = sm.sol + e * N;
-  sm.scr = flat ? sm.state + 2 * e * W : nullptr;
+  sm.coefA = base + o.coefA;
+  sm.coefB = base + o.coefB;
+  sm.xs = base + o.xs;
+  sm.sx = base + o.sx;
+  sm.sol = base + o.sol;
+  sm.state = base + o.state;
+  sm.scr = flat ? base + o.scr : nullptr;
+  const bool mixed = !std::is_same<R, RL>::value;
+  sm.coefH = mixed ? base + o.coefH : nullptr;
+  sm.xsH = mixed ? base + o.xsH : nullptr;
+  sm.xst = mixed ? sm.xsH : sm.xs;
   return sm;
 }
 
@@ -608,13 +739,16 @@ __device__ __forceinline__ cx<R> load_cx(const void* base, bool f64, long long i
 // the 64 registers spill), N = 6 flat within noise, N = 12 at 5 (generalized
 // 3-view 5360 vs 5326 hyp/s at 4, uncalibrated trifocal 1376 vs 1348; 6 and 7
 // spill), N = 30 at 3 (406 vs 397 at 4); FP32 N = 12 at 7, N = 30 at 5 (577
-// vs 552 at 3).  Variant 1 is the runner-up budget.
-template <int N, typename R, int V>
+// vs 552 at 3).  Variant 1 is the runner-up budget.  The mixed tracker (FP64 state, FP32
+// linear algebra) holds the row in FP32 and asks for about the FP32 budget.
+template <int N, typename R, typename RL, int V>
 constexpr int track_min_blocks() {
-  return V == 0 ? (sizeof(R) == 8 ? (N <= 4 ? 6 : N <= 8 ? 4 : N <= 12 ? 5 : 3)
-                                  : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 5))
-                : (sizeof(R) == 8 ? (N <= 4 ? 8 : N <= 8 ? 6 : N <= 12 ? 4 : N <= 18 ? 4 : 2)
-                                  : (N <= 8 ? 10 : N <= 12 ? 8 : N <= 18 ? 5 : 4));
+  return !std::is_same<R, RL>::value
+             ? (V == 0 ? (N <= 8 ? 6 : N <= 12 ? 6 : N <= 18 ? 4 : 4) : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 5 : 3))
+         : V == 0 ? (sizeof(R) == 8 ? (N <= 4 ? 6 : N <= 8 ? 4 : N <= 12 ? 5 : 3)
+                                    : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 5))
+                  : (sizeof(R) == 8 ? (N <= 4 ? 8 : N <= 8 ? 6 : N <= 12 ? 4 : N <= 18 ? 4 : 2)
+                                    : (N <= 8 ? 10 : N <= 12 ? 8 : N <= 18 ? 5 : 4));
 }
 
 __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64_t* g_hx, const uint16_t* g_hxo,
@@ -638,7 +772,9 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 }
 
 // -------------------------------------------------------------------------------------------------
-// the tracker kernel, one precision R for the whole path
+// the tracker kernel: state, step control and norms in precision R, H_x, H_t and the LU in RL
+// (R = RL: the plain FP64 and FP32 trackers; R = double, RL = float: the mixed tracker, whose
+// corrector evaluates its residual H in R, so its endpoints converge to FP64 accuracy)
 //
 // Each sub-warp runs its path as a small state machine (phase 0..3 = RK stage,
 // 4 = Newton iteration).  One trip of the warp loop performs exactly one
@@ -654,12 +790,12 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 // with step dt_in[i] and the step / corrector counts already in steps / corr.
 // -------------------------------------------------------------------------------------------------
 #ifdef GHC_TRACK_MIN_BLOCKS
-#define GHC_MINB(N, R, V) GHC_TRACK_MIN_BLOCKS
+#define GHC_MINB(N, R, RL, V) GHC_TRACK_MIN_BLOCKS
 #else
-#define GHC_MINB(N, R, V) track_min_blocks<N, R, V>()
+#define GHC_MINB(N, R, RL, V) track_min_blocks<N, R, RL, V>()
 #endif
-template <typename R, int N, int W, int KIND, int V, int S>
-__global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const TrackParams p) {
+template <typename R, typename RL, int N, int W, int KIND, int V, int S>
+__global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const TrackParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Tables tb = stage_tables(smem, p.hx_terms, p.hx_off, p.ht_terms, p.ht_off, N, p.n_hx_terms, p.n_ht_terms);
 
@@ -669,9 +805,10 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int walk = (kFlatAlways<N> && p.flat_eval == 0) ? 1 : p.flat_eval;
   const bool flat = walk != 0;
-  SubMem sm = sub_layout<R>(smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) +
-                                (size_t)g * sub_bytes(N, Mc, W, flat ? p.scr_slots : 0, (int)sizeof(cx<R>)),
-                            N, Mc, W, flat);
+  SubMem sm = sub_layout<R, RL>(smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) +
+                                    (size_t)g * sub_bytes(N, Mc, W, flat ? p.scr_slots : 0, (int)sizeof(cx<RL>),
+                                                          (int)sizeof(cx<R>)),
+                                N, Mc, W, p.scr_slots, flat);
   sm.nz = row_mask<N>(tb.hx_off, l);
   sm.walk = walk;
   // this lane's RK base point x0 and accumulator sols live in shared memory (register relief)
@@ -700,6 +837,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
   R t0 = 0, dt = 0, t_step = 0, half = 0, dt_pre = 0;
   R coef_t = R(-1);  // the t at which this sub-warp's coefficient buffers hold c_k(t) (-1: none)
   bool end_zone = false, success = false, inf = false, finished = false;
+  bool step_ill = false, ill_stop = false;  // mixed: a solve of this step was ill-conditioned; stop after it
   int nsucc = 0, step = 0, ncorr = 0, phase = 0, cit = 0, nfail = 0;
   const R dt_init = (KIND == KIND_PH) ? R(0.01) : R(0.05);
 
@@ -719,11 +857,13 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
     half = f_mul(R(0.5), dt);
     phase = 0;
     cit = 0;
+    step_ill = false;
   };
   // the path stops before its next step (kernel_HC_Solver_P3P.cu:247-249, plus the handover rules)
   auto at_end = [&]() -> bool {
     return !(t0 < R(1) && f_sub(R(1), t0) > R(1e-7)) || step > p.max_steps ||
-           (p.t_handover > 0.0 && f_sub(t_hand, t0) <= R(1e-6)) || (p.fail_limit > 0 && nfail >= p.fail_limit);
+           (p.t_handover > 0.0 && f_sub(t_hand, t0) <= R(1e-6)) || (p.fail_limit > 0 && nfail >= p.fail_limit) ||
+           ill_stop;
   };
   auto init_path = [&](long long it) {
     hyp = it / p.paths_per_hyp;
@@ -750,6 +890,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
     inf = false;
     nsucc = 0;
     nfail = 0;
+    step_ill = ill_stop = false;
     finished = at_end();
     if (!finished) prologue();
   };
@@ -777,7 +918,8 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
     rec_i[3] = cit;
     rec_i[4] = nfail;
     rec_i[5] = nsucc;
-    rec_i[6] = (alive ? 1 : 0) | (finished ? 2 : 0) | (end_zone ? 4 : 0) | (success ? 8 : 0) | (inf ? 16 : 0);
+    rec_i[6] = (alive ? 1 : 0) | (finished ? 2 : 0) | (end_zone ? 4 : 0) | (success ? 8 : 0) | (inf ? 16 : 0) |
+               (step_ill ? 32 : 0) | (ill_stop ? 64 : 0);
   };
   auto unstash = [&]() {
     t0 = rec_r[0];
@@ -800,7 +942,9 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
     end_zone = (f >> 2) & 1;
     success = (f >> 3) & 1;
     inf = (f >> 4) & 1;
-    const volatile cx<R>* xv = reinterpret_cast<const volatile cx<R>*>(sm.xs);
+    step_ill = (f >> 5) & 1;
+    ill_stop = (f >> 6) & 1;
+    const volatile cx<R>* xv = reinterpret_cast<const volatile cx<R>*>(sm.xst);
     x = (l < N) ? mk(xv[l].re, xv[l].im) : mk(R(0), R(0));
   };
 
@@ -812,15 +956,17 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
     // (RK stages 2 and 3 share t + dt/2, and after an accepted step the next step starts at the t
     // of the last stage, whose coefficients are still in the buffers: evaluate only on a new t)
     if (rk && t0 != coef_t) {
-      coef_eval<R, W, KIND>(p, sm, hyp, t0, l);
+      coef_eval<R, RL, W, KIND>(p, sm, hyp, t0, l);
       coef_t = t0;
     }
     // ---------------- one evaluate-and-solve per sub-warp (predictor: -H_t, corrector: H)
-    write_track<R, N>(sm, l, x);
+    write_track<R, RL, N>(sm, l, x);
     stash();
     __syncwarp(kFull);
-    const cx<R> v = eval_solve<R, N, W, KIND, S>(tb, sm, l, rk ? 1 : 0);
+    bool ill = false;
+    const cx<R> v = eval_solve<R, RL, N, W, KIND, S>(tb, sm, l, rk ? 1 : 0, p.cond_limit, ill);
     unstash();
+    if (served && ill) step_ill = true;
     // ---------------- corrector norms (kernel_HC_Solver_P3P.cu:204-219), all lanes take part
     R ns0 = 0, nc0 = 0;
     if (__any_sync(kFull, corr)) {
@@ -886,6 +1032,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, V)) track_kernel(const Tra
         }
       }
       ++step;
+      if (step_ill) ill_stop = true;
       if (!done) done = at_end();
       if (done && !inf && p.t_handover > 0.0 && f_sub(t_hand, t0) <= R(1e-6) && step <= p.max_steps &&
           dt < dt_pre)
@@ -939,9 +1086,9 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int walk = (kFlatAlways<N> && p.flat_eval == 0) ? 1 : p.flat_eval;
   const bool flat = walk != 0;
-  SubMem sm = sub_layout<double>(
-      smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + (size_t)g * sub_bytes(N, Mc, W, flat ? p.scr_slots : 0, 16),
-      N, Mc, W, flat);
+  SubMem sm = sub_layout<double, double>(smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) +
+                                             (size_t)g * sub_bytes(N, Mc, W, flat ? p.scr_slots : 0, 16, 16),
+                                         N, Mc, W, p.scr_slots, flat);
   sm.nz = row_mask<N>(tb.hx_off, l);
   sm.walk = walk;
   const int subs_per_cta = blockDim.x / W;
@@ -956,26 +1103,28 @@ __global__ void __launch_bounds__(128) polish_kernel(const PolishParams p) {
     cx<double> x = (valid && l < N) ? mk(ep[2 * l], ep[2 * l + 1]) : mk(0.0, 0.0);
     if (conv) {
       if (KIND == KIND_P2C) {
-        coef_eval_p2c<double, W>(p.coef_hx + 2 * hyp * p.stride_hx, p.coef_ht + 2 * hyp * p.stride_ht, p.M, p.K,
-                                 1.0, view<double>(sm.coefA), view<double>(sm.coefB), l);
+        coef_eval_p2c<double, double, W, false>(p.coef_hx + 2 * hyp * p.stride_hx, p.coef_ht + 2 * hyp * p.stride_ht,
+                                                p.M, p.K, 1.0, view<double>(sm.coefA), view<double>(sm.coefB),
+                                                nullptr, l);
       } else {
-        coef_eval_ph<double, W>(p.p_start, p.p_tgt + 2 * hyp * p.stride_p, p.p_diff + 2 * hyp * p.stride_p, p.P,
-                                1.0, view<double>(sm.coefA), view<double>(sm.coefB), l);
+        coef_eval_ph<double, double, W, false>(p.p_start, p.p_tgt + 2 * hyp * p.stride_p,
+                                               p.p_diff + 2 * hyp * p.stride_p, p.P, 1.0, view<double>(sm.coefA),
+                                               view<double>(sm.coefB), nullptr, l);
       }
     }
     __syncwarp(kFull);
     for (int it = 0; it < p.iters; ++it) {
-      write_track<double, N>(sm, l, x);
+      write_track<double, double, N>(sm, l, x);
       __syncwarp(kFull);
-      const cx<double> d = eval_solve<double, N, W, KIND, S>(tb, sm, l, 0);
+      const cx<double> d = eval_solve<double, double, N, W, KIND, S>(tb, sm, l, 0);
       if (conv) x = c_sub(x, d);
     }
     // residual |H(x,1)|
-    write_track<double, N>(sm, l, x);
+    write_track<double, double, N>(sm, l, x);
     __syncwarp(kFull);
     cx<double> A[N];
     cx<double> h;
-    eval_any<double, N, W, KIND, S>(tb, sm, l, A, h, 0);
+    eval_any<double, double, N, W, KIND, S>(tb, sm, l, A, h, 0);
     const double s = tree_sum<double, N, W>(l < N ? c_abs2(h) : 0.0);
     const double s0 = __shfl_sync(kFull, s, leader);
     if (valid) {

@@ -2,5 +2,5 @@
 #include "tracker_launch.cuh"
 
 namespace ghc {
-int launch_track_fp32_v0(const TrackParams& p, cudaStream_t s, int n_sm) { return launch_mode<float, 0>(p, s, n_sm); }
+int launch_track_fp32_v0(const TrackParams& p, cudaStream_t s, int n_sm) { return launch_mode<float, float, 0>(p, s, n_sm); }
 }  // namespace ghc

@@ -12,15 +12,15 @@ namespace launch_detail {
 
 constexpr int kBlock = 128;
 
-template <typename R, int N, int KIND, int V, int S>
+template <typename R, typename RL, int N, int KIND, int V, int S>
 int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
   constexpr int W = (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
-  auto kern = dev::track_kernel<R, N, W, KIND, V, S>;
+  auto kern = dev::track_kernel<R, RL, N, W, KIND, V, S>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
   const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
-  const size_t smem =
-      dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, slots, 2 * (int)sizeof(R));
+  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) +
+                      subs * dev::sub_bytes(N, Mc, W, slots, 2 * (int)sizeof(RL), 2 * (int)sizeof(R));
   // Host calls in the launch path delay small launches, so per instantiation and device the
   // shared-memory attribute is only ever raised (to the largest size asked for, so a concurrent
   // launch never sees it below its own size) and the occupancy of the last size is kept.
@@ -65,15 +65,15 @@ int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
   return e == cudaSuccess ? 0 : -23;
 }
 
-template <typename R, int N, int KIND, int V>
+template <typename R, typename RL, int N, int KIND, int V>
 int launch_track_t(const TrackParams& p, cudaStream_t s, int n_sm) {
   switch (p.shape) {
     case EVAL_1_2:
-      return launch_track_s<R, N, KIND, V, EVAL_1_2>(p, s, n_sm);
+      return launch_track_s<R, RL, N, KIND, V, EVAL_1_2>(p, s, n_sm);
     case EVAL_2_3:
-      return launch_track_s<R, N, KIND, V, EVAL_2_3>(p, s, n_sm);
+      return launch_track_s<R, RL, N, KIND, V, EVAL_2_3>(p, s, n_sm);
     default:
-      return launch_track_s<R, N, KIND, V, EVAL_GENERAL>(p, s, n_sm);
+      return launch_track_s<R, RL, N, KIND, V, EVAL_GENERAL>(p, s, n_sm);
   }
 }
 
@@ -84,7 +84,8 @@ int launch_polish_s(const PolishParams& p, cudaStream_t s) {
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int subs = kBlock / W;
   const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
-  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, slots, 16);
+  const size_t smem =
+      dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, slots, 16, 16);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -20;
   long long grid = (p.n_items + subs - 1) / subs;
   if (grid > 65535LL * 16) grid = 65535LL * 16;
@@ -110,36 +111,42 @@ int launch_polish_t(const PolishParams& p, cudaStream_t s) {
 
 #define GHC_P2C_SIZES(X) X(3) X(4) X(5) X(6) X(8) X(10) X(11) X(12) X(16) X(18)
 
-// dispatch of one precision mode over the compiled sizes
-template <typename R, int V>
+// dispatch of one precision mode (state R, linear algebra RL) over the compiled sizes
+template <typename R, typename RL, int V>
 int launch_mode(const TrackParams& p, cudaStream_t s, int n_sm) {
   using namespace launch_detail;
   if (p.kind == KIND_P2C) {
     switch (p.N) {
 #define CASE(n) \
   case n:       \
-    return launch_track_t<R, n, KIND_P2C, V>(p, s, n_sm);
+    return launch_track_t<R, RL, n, KIND_P2C, V>(p, s, n_sm);
       GHC_P2C_SIZES(CASE)
 #undef CASE
       default:
         return -10;
     }
   }
-  if (p.kind == KIND_PH && p.N == 30) return launch_track_t<R, 30, KIND_PH, V>(p, s, n_sm);
+  if (p.kind == KIND_PH && p.N == 30) return launch_track_t<R, RL, 30, KIND_PH, V>(p, s, n_sm);
   return -10;
 }
 
 // one translation unit per (precision, variant): tracker_fp64.cu, tracker_fp64_v1.cu, tracker_fp32.cu,
-// tracker_fp32_v1.cu; launch_track_fp64 / _fp32 (tracker.cu) pick by TrackParams::variant
+// tracker_fp32_v1.cu, tracker_mixed.cu, tracker_mixed_v1.cu; launch_track_fp64 / _fp32 / _mixed
+// (tracker.cu) pick by TrackParams::variant
 int launch_track_fp64_v0(const TrackParams& p, cudaStream_t s, int n_sm);
 int launch_track_fp64_v1(const TrackParams& p, cudaStream_t s, int n_sm);
 int launch_track_fp32_v0(const TrackParams& p, cudaStream_t s, int n_sm);
 int launch_track_fp32_v1(const TrackParams& p, cudaStream_t s, int n_sm);
+int launch_track_mixed_v0(const TrackParams& p, cudaStream_t s, int n_sm);
+int launch_track_mixed_v1(const TrackParams& p, cudaStream_t s, int n_sm);
 inline int launch_track_fp64(const TrackParams& p, cudaStream_t s, int n_sm) {
   return p.variant ? launch_track_fp64_v1(p, s, n_sm) : launch_track_fp64_v0(p, s, n_sm);
 }
 inline int launch_track_fp32(const TrackParams& p, cudaStream_t s, int n_sm) {
   return p.variant ? launch_track_fp32_v1(p, s, n_sm) : launch_track_fp32_v0(p, s, n_sm);
+}
+inline int launch_track_mixed(const TrackParams& p, cudaStream_t s, int n_sm) {
+  return p.variant ? launch_track_mixed_v1(p, s, n_sm) : launch_track_mixed_v0(p, s, n_sm);
 }
 
 }  // namespace ghc

@@ -36,7 +36,7 @@ class ProblemInfo(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 96), ("kind", _I32), ("N", _I32), ("P", _I32), ("M", _I32), ("K", _I32),
                 ("paths", _I32), ("Tx", _I32), ("Px", _I32), ("Tt", _I32), ("Pt", _I32), ("max_steps", _I32),
                 ("max_corr", _I32), ("incr_steps", _I32), ("n_hx_terms", _I32), ("n_ht_terms", _I32),
-                ("has_p2c_terms", _I32), ("subwarp", _I32)]
+                ("has_p2c_terms", _I32), ("subwarp", _I32), ("device", _I32)]
 
 
 class Counts(ctypes.Structure):
@@ -55,7 +55,7 @@ class TrackArgs(ctypes.Structure):
                 ("d_start_sols", _P), ("d_coef_hx", _P), ("d_coef_ht", _P), ("d_p_start", _P),
                 ("d_p_target", _P), ("d_p_diff", _P), ("d_endpoints", _P), ("d_status", _P), ("d_conv", _P),
                 ("d_inf", _P), ("d_steps", _P), ("d_corr", _P), ("d_t_end", _P), ("d_dt_end", _P),
-                ("d_resid", _P), ("d_counter", _P), ("paths", _I32)]
+                ("d_resid", _P), ("d_counter", _P), ("paths", _I32), ("cond_limit", ctypes.c_double)]
 
 
 def _sig(name, res, args):
@@ -143,6 +143,12 @@ class Problem:
                 setattr(self, f, getattr(info, f))
         self.name = info.name.decode()
 
+    def device(self):
+        """Device holding the handle's compiled tables (uploaded by its first tracking call), -1: none."""
+        info = ProblemInfo()
+        _check(ghc_problem_get_info(self.h, ctypes.byref(info)), "ghc_problem_get_info")
+        return info.device
+
     def __del__(self):
         h = getattr(self, "h", None)
         if h and ghc_problem_free is not None:
@@ -220,15 +226,18 @@ class Workspace:
 
 
 def track(pb, ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, d_p_target=None, d_p_diff=None,
-          t_switch=0.9, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False, step=None,
-          no_alloc=False):
+          t_switch=1.0, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False, step=None,
+          no_alloc=False, cond_limit=0.0):
     """Launch the batched tracker (asynchronous on torch's current stream).
 
     step: optional dict(corr_tol2=, first_tol2=, dt_max=) step control; the
     default is the reference's (see ROBUST_STEP for the path-jump-free one).
+    PREC_MIXED: the mixed tracker (FP64 state and residual, FP32 H_x, H_t and LU) for
+    t < t_switch (>= 1: the whole path), then FP64 for the paths it hands over
+    (cond_limit: pivot-magnitude span of an FP32 solve that hands a path over, 0: 1e4).
     """
     a = _track_args(ws, d_start_sols, d_coef_hx, d_coef_ht, d_p_start, d_p_target, d_p_diff, t_switch,
-                    polish_iters, max_steps, max_corr, incr_steps, want_resid, step)
+                    polish_iters, max_steps, max_corr, incr_steps, want_resid, step, cond_limit)
     if no_alloc:
         # ghc_track_noalloc: counter and tables in the library's fixed device array
         a.d_counter = None
@@ -261,7 +270,8 @@ def get_tuning(pb, precision):
 
 
 def _track_args(ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, d_p_target=None, d_p_diff=None,
-                t_switch=0.9, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False, step=None):
+                t_switch=1.0, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False, step=None,
+                cond_limit=0.0):
     a = TrackArgs()
     a.n_hyp = ws.n_hyp
     a.precision = ws.precision
@@ -282,6 +292,7 @@ def _track_args(ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None
     a.d_resid = ws.resid.data_ptr() if (want_resid or polish_iters > 0) and ws.precision != PREC_FP32 else None
     a.d_counter = ws.counter.data_ptr()
     a.paths = ws.paths
+    a.cond_limit = cond_limit
     return a
 
 
@@ -344,7 +355,7 @@ def solve_outputs(pb, n_hyp):
                 ms=np.zeros(3))
 
 
-def solve_host(pb, precision=PREC_FP64, targets=None, t_switch=0.9, polish_iters=0, out=None):
+def solve_host(pb, precision=PREC_FP64, targets=None, t_switch=1.0, polish_iters=0, out=None):
     """One-call host solve (host buffers in and out, copies included).
 
     targets: [n_hyp, P+1] complex (None: the problem's target, n_hyp = 1).  out: arrays from

@@ -73,7 +73,7 @@ class Batch:
         self.paths = s0.shape[0]
         self.d_sols = _cx(s0, torch, torch.float32 if precision == ghc.PREC_FP32 else None)
         self.ws = ghc.Workspace(self.pb, H, precision, paths=self.paths)
-        self.kw = dict(polish_iters=polish, want_resid=polish > 0, t_switch=0.9)
+        self.kw = dict(polish_iters=polish, want_resid=polish > 0)
         if step:
             self.kw.update(step)
 

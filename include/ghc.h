@@ -34,7 +34,7 @@ extern "C" {
 
 #define GHC_PREC_FP64 0  /* plain FP64 tracker */
 #define GHC_PREC_FP32 1  /* reference precision (complex FP32) */
-#define GHC_PREC_MIXED 2 /* FP32 tracking to t_switch (early handover on failure), FP64 from there */
+#define GHC_PREC_MIXED 2 /* FP64 state and residual with FP32 H_x, H_t and LU; FP64 after ill-conditioning */
 
 #define GHC_STATUS_CONVERGED 0
 #define GHC_STATUS_DIVERGED 1 /* |x|^2 > 1e14 in the corrector ("infinity") */
@@ -52,6 +52,8 @@ typedef struct {
   int32_t n_hx_terms, n_ht_terms;      /* non-padding monomial terms */
   int32_t has_p2c_terms;               /* p2c_terms.txt present (host/device P2C available) */
   int32_t subwarp;                     /* lanes per path on the GPU */
+  int32_t device;                      /* device holding the handle's compiled tables and work counter
+                                          (uploaded by its first tracking call), -1: none */
 } ghc_problem_info;
 
 /* Result counts of one hypothesis. */
@@ -118,9 +120,12 @@ typedef struct {
   int32_t max_steps;          /* <= 0: YAML value */
   int32_t max_corr;           /* <= 0: YAML value */
   int32_t incr_steps;         /* <= 0: YAML value */
-  double t_switch;            /* GHC_PREC_MIXED: FP32 tracker for t < t_switch (at most 0.95; <= 0: all FP64);
-                                 a path failing 2 steps in a row or diverging goes FP64 at its last
-                                 accepted point; needs d_steps, d_corr, d_t_end, d_dt_end */
+  double t_switch;            /* GHC_PREC_MIXED: the mixed tracker (FP64 track, t, step control and corrector
+                                 residual H; FP32 H_x, H_t and LU) for t < t_switch (>= 1: to t = 1;
+                                 <= 0: all FP64); a path goes on in FP64 after a step whose FP32 solve had
+                                 pivot magnitudes spanning more than cond_limit, after 4 failed steps in a
+                                 row, or on divergence (at its last accepted point); needs d_steps, d_corr,
+                                 d_t_end, d_dt_end */
   int32_t polish_iters;       /* Newton iterations at t = 1 after tracking (FP64 state only) */
   /* step control; <= 0 selects the reference's value (kernel_HC_Solver_P3P.cu:214) */
   double corr_tol2;           /* corrector success |dx|^2 < corr_tol2 |x|^2 (reference 1e-6) */
@@ -147,6 +152,9 @@ typedef struct {
   int32_t* d_counter;         /* one int of device memory (work-stealing counter) */
   /* start solutions per hypothesis in d_start_sols; <= 0: the problem's Num_Of_Tracks */
   int32_t paths;
+  /* GHC_PREC_MIXED: the pivot-magnitude span max|U_ii| / min|U_ii| of an FP32 solve above which the
+     path goes on in FP64 (<= 0: 1e4) */
+  double cond_limit;
 } ghc_track_args;
 
 int ghc_track(const ghc_problem* pb, const ghc_track_args* args, void* stream);

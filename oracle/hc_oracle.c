@@ -6,7 +6,8 @@
  * the checker.  The product never links or calls it.
  *
  * The precision-generic body lives in hc_oracle_body.h and is instantiated
- * for double (suffix _d) and float (suffix _f).  Build flags (oracle/build.py):
+ * for double (suffix _d), float (suffix _f), and the mixed tracker's first phase
+ * (suffix _m: double state, float linear algebra).  Build flags (oracle/build.py):
  * -O2 -ffp-contract=off -fopenmp, so no multiply-add is fused except through
  * the explicit fma()/fmaf() calls.
  */
@@ -45,6 +46,9 @@ typedef struct {
   double t_handover;
   int32_t fail_limit;
   int32_t resume;
+  /* mixed tracker: hand a path over after a step in which a float solve's pivot magnitudes spanned
+   * more than cond_limit (0: never) */
+  double cond_limit;
 } orc_problem;
 
 typedef struct {
@@ -72,6 +76,20 @@ typedef struct {
 #undef SUFFIX
 #undef FMA
 #undef FABS
+
+/* the mixed tracker's first phase (the tracker library's GHC_PREC_MIXED, not a reference feature):
+ * double state, step control, norms and corrector residual, with H_x, H_t and the LU in float */
+#define ORC_MIXED_LA 1
+#define REAL double
+#define SUFFIX _m
+#define FMA fma
+#define FABS fabs
+#include "hc_oracle_body.h"
+#undef REAL
+#undef SUFFIX
+#undef FMA
+#undef FABS
+#undef ORC_MIXED_LA
 
 int orc_abi_version(void) { return 1; }
 int orc_sizeof_problem(void) { return (int)sizeof(orc_problem); }

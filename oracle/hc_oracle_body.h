@@ -98,6 +98,9 @@ typedef struct {
   /* PH: parameter homotopy values at t and parameter differences */
   CX ph[ORC_MMAX];
   CX dp[ORC_MMAX];
+#ifdef ORC_MIXED_LA
+  coefs__f lo; /* the same values rounded to float, for H_x, H_t and the float LU */
+#endif
 } SFX(coefs_);
 #define COEFS SFX(coefs_)
 
@@ -141,6 +144,19 @@ static void SFX(eval_coefs)(const HYP* h, REAL t, COEFS* cf) {
     cf->ph[P] = SFX(c_make)(1, 0);
     cf->dp[P] = h->p_diff[P];
   }
+#ifdef ORC_MIXED_LA
+  /* mixed: every coefficient computed in double, then rounded once to float */
+  const int nk = (pb->kind == ORC_P2C) ? pb->M + 1 : pb->P + 1;
+  for (int k = 0; k < nk; ++k) {
+    if (pb->kind == ORC_P2C) {
+      cf->lo.c[k] = c_make_f((float)cf->c[k].re, (float)cf->c[k].im);
+      cf->lo.cp[k] = c_make_f((float)cf->cp[k].re, (float)cf->cp[k].im);
+    } else {
+      cf->lo.ph[k] = c_make_f((float)cf->ph[k].re, (float)cf->ph[k].im);
+      cf->lo.dp[k] = c_make_f((float)cf->dp[k].re, (float)cf->dp[k].im);
+    }
+  }
+#endif
 }
 
 /* Row r of H_x into A[0..N) */
@@ -207,7 +223,7 @@ static CX SFX(eval_h_row)(const orc_problem* pb, const COEFS* cf, const CX* x, i
  * variable order.  trace (optional): piv[i] = the pivot position of column i, and
  * mags[i*N + j] = |Re|+|Im| of the row at position j (j >= i) when column i was searched.
  */
-static void SFX(lu_solve_trace)(int N, CX A[][ORC_NMAX], CX* b, CX* z, int32_t* piv, REAL* mags) {
+static void SFX(lu_solve_trace)(int N, CX A[][ORC_NMAX], CX* b, CX* z, int32_t* piv, REAL* mags, REAL* piv_range) {
   int pos[ORC_NMAX], row_at[ORC_NMAX];
   CX myrcp[ORC_NMAX];
   for (int r = 0; r < N; ++r) pos[r] = row_at[r] = r;
@@ -224,6 +240,11 @@ static void SFX(lu_solve_trace)(int N, CX A[][ORC_NMAX], CX* b, CX* z, int32_t* 
       }
     }
     if (piv) piv[i] = best_pos;
+    if (piv_range) { /* the pivot magnitudes' range (|U_ii| as |Re|+|Im|) and whether one was NaN */
+      if (i == 0 || best < piv_range[0]) piv_range[0] = best;
+      if (i == 0 || best > piv_range[1]) piv_range[1] = best;
+      if (best != best) piv_range[2] = 1;
+    }
     const int best_r = row_at[best_pos];
     /* zero pivot: the pivot row's own magnitude is exactly 0 */
     const int zero = (best == (REAL)0);
@@ -257,11 +278,37 @@ static void SFX(lu_solve_trace)(int N, CX A[][ORC_NMAX], CX* b, CX* z, int32_t* 
   }
 }
 
-static void SFX(lu_solve)(int N, CX A[][ORC_NMAX], CX* b, CX* z) { SFX(lu_solve_trace)(N, A, b, z, NULL, NULL); }
+static void SFX(lu_solve)(int N, CX A[][ORC_NMAX], CX* b, CX* z) { SFX(lu_solve_trace)(N, A, b, z, NULL, NULL, NULL); }
 
 /* one evaluation + solve: z = H_x^{-1} * rhs; rhs = -H_t (which=1) or H (which=0) */
-static void SFX(eval_solve)(const orc_problem* pb, const COEFS* cf, const CX* x, int which, CX* z) {
+static void SFX(eval_solve)(const orc_problem* pb, const COEFS* cf, const CX* x, int which, CX* z, int* ill) {
   const int N = pb->N;
+  (void)ill;
+#ifdef ORC_MIXED_LA
+  /* mixed: H_x and -H_t in float from the float coefficients and the track rounded to float; the
+   * corrector's residual H in double, rounded to float; the LU in float; the step back in double */
+  {
+    cx__f xf[ORC_NMAX + 1], A[ORC_NMAX][ORC_NMAX], b[ORC_NMAX], zf[ORC_NMAX];
+    for (int r = 0; r < N; ++r) xf[r] = c_make_f((float)x[r].re, (float)x[r].im);
+    xf[N] = c_make_f(1, 0);
+    for (int r = 0; r < N; ++r) {
+      eval_hx_row_f(pb, &cf->lo, xf, r, A[r]);
+      if (which) {
+        const cx__f h = eval_h_row_f(pb, &cf->lo, xf, r, 1);
+        b[r] = c_make_f(-h.re, -h.im);
+      } else {
+        const CX h = SFX(eval_h_row)(pb, cf, x, r, 0);
+        b[r] = c_make_f((float)h.re, (float)h.im);
+      }
+    }
+    float range[3] = {0, 0, 0};
+    lu_solve_trace_f(N, A, b, zf, NULL, NULL, range);
+    for (int r = 0; r < N; ++r) z[r] = SFX(c_make)((double)zf[r].re, (double)zf[r].im);
+    /* ill-conditioned for the float solve: the pivot magnitudes span more than cond_limit (or NaN) */
+    if (pb->cond_limit > 0 && ill && (range[2] != 0 || !(range[1] <= (float)pb->cond_limit * range[0]))) *ill = 1;
+    return;
+  }
+#endif
   CX A[ORC_NMAX][ORC_NMAX];
   CX b[ORC_NMAX];
   for (int r = 0; r < N; ++r) {
@@ -304,6 +351,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
   static const REAL frac[3] = {(REAL)0.5, (REAL)0.5, (REAL)1.0};
 
   REAL dt_pre = dt; /* the step without the handover clamp: the next phase resumes with it */
+  int ill = 0, ill_stop = 0; /* mixed: a solve of this step was ill-conditioned for float; stop after it */
   for (int step = steps; step <= pb->max_steps; ++step) {
     if (!(t0 < (REAL)1 && (REAL)1 - t0 > (REAL)1e-7)) break;
     if (pb->t_handover > 0 && t_hand - t0 <= (REAL)1e-6) {
@@ -311,7 +359,9 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
       break;
     }
     if (pb->fail_limit > 0 && nfail >= pb->fail_limit) break;
+    if (ill_stop) break;
     ++steps;
+    ill = 0;
     /* end-zone step clamp (kernel_HC_Solver_P3P.cu:121-131; PH edge 0.95 at trifocal_2op1p_30x30.cu:163-182) */
     if (!end_zone && FABS((REAL)1 - t0) <= (REAL)0.0500001) end_zone = 1;
     if (end_zone) {
@@ -328,7 +378,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
     /* loopy RK4 predictor (kernel_HC_Solver_P3P.cu:139-183) */
     for (int rk = 0; rk < 4; ++rk) {
       SFX(eval_coefs)(h, t0, cf);
-      SFX(eval_solve)(pb, cf, x, 1, k);
+      SFX(eval_solve)(pb, cf, x, 1, k, &ill);
       if (rk < 3) {
         const REAL a = dt * wgt[rk];
         const REAL d = dt * frac[rk];
@@ -352,7 +402,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
     inf = 0;
     for (int it = 0; it < pb->max_corr; ++it) {
       ++corr;
-      SFX(eval_solve)(pb, cf, x, 0, k);
+      SFX(eval_solve)(pb, cf, x, 0, k, &ill);
       REAL ns[ORC_NMAX], nc[ORC_NMAX];
       for (int r = 0; r < N; ++r) {
         x[r] = SFX(c_sub)(x[r], k[r]);
@@ -390,6 +440,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
         if ((double)dt > pb->dt_max) dt = (REAL)pb->dt_max;
       }
     }
+    if (ill) ill_stop = 1;
   }
 
   const int conv = (t0 >= (REAL)1 || ((REAL)1 - t0 <= (REAL)1e-7));
@@ -407,7 +458,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
   if (conv) {
     SFX(eval_coefs)(h, (REAL)1, cf);
     for (int it = 0; it < pb->polish_iters; ++it) {
-      SFX(eval_solve)(pb, cf, x, 0, k);
+      SFX(eval_solve)(pb, cf, x, 0, k, NULL);
       for (int r = 0; r < N; ++r) x[r] = SFX(c_sub)(x[r], k[r]);
     }
     REAL hr[ORC_NMAX];
@@ -502,7 +553,7 @@ int SFX(orc_lu_pivots)(int32_t N, const REAL* A_rowmajor, const REAL* b, REAL* z
     for (int c = 0; c < N; ++c) A[r][c] = SFX(c_make)(A_rowmajor[2 * (r * N + c)], A_rowmajor[2 * (r * N + c) + 1]);
     bb[r] = SFX(c_make)(b[2 * r], b[2 * r + 1]);
   }
-  SFX(lu_solve_trace)(N, A, bb, zz, piv, mags);
+  SFX(lu_solve_trace)(N, A, bb, zz, piv, mags, NULL);
   for (int r = 0; r < N; ++r) {
     z[2 * r] = zz[r].re;
     z[2 * r + 1] = zz[r].im;

@@ -212,7 +212,8 @@ class _Prob(ctypes.Structure):
                 ("incr_steps", ctypes.c_int32), ("polish_iters", ctypes.c_int32),
                 ("hx_idx", ctypes.c_void_p), ("ht_idx", ctypes.c_void_p), ("corr_tol2", ctypes.c_double),
                 ("first_tol2", ctypes.c_double), ("dt_max", ctypes.c_double),
-                ("t_handover", ctypes.c_double), ("fail_limit", ctypes.c_int32), ("resume", ctypes.c_int32)]
+                ("t_handover", ctypes.c_double), ("fail_limit", ctypes.c_int32), ("resume", ctypes.c_int32),
+                ("cond_limit", ctypes.c_double)]
 
 # step control of the reference (kernel_HC_Solver_P3P.cu:214, no contraction test, no dt cap)
 REFERENCE_STEP = dict(corr_tol2=1e-6, first_tol2=float("inf"), dt_max=float("inf"))
@@ -257,21 +258,24 @@ def _prob_struct(pb, polish_iters, max_steps=None, max_corr=None, incr=None, ste
     return s
 
 
-# the tracker library's two-phase mixed precision (csrc/tracker.cu): float tracking to
-# min(t_switch, 0.95), a path handed over after 2 failed steps in a row or on divergence
-MIXED_FAIL_LIMIT = 2
-MIXED_MAX_SWITCH = 0.95
-MIXED_F32_TOL2 = 1e-9  # the float phase's corrector tolerance floor
+# the tracker library's two-phase mixed precision (csrc/tracker.cu): the mixed tracker (double state,
+# residual and step control, float H_x, H_t and LU) to t = 1 or t_switch < 1, a path handed over after
+# a step whose float solve had pivot magnitudes spanning more than cond_limit, after 4 failed steps in
+# a row, or on divergence; then the double tracker resumes every path
+MIXED_FAIL_LIMIT = 4
+MIXED_COND_LIMIT = 1e4
 
 
 def track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precision="d",
-          polish_iters=0, nthreads=0, max_steps=None, max_corr=None, incr=None, step=None, t_switch=0.9):
+          polish_iters=0, nthreads=0, max_steps=None, max_corr=None, incr=None, step=None, t_switch=1.0,
+          cond_limit=MIXED_COND_LIMIT):
     """Track all start paths for H hypotheses.
 
     P2C: hx [H, (M+1)(K+1)], ht [H, (M+1)K] complex.
     PH:  p_start [P+1], p_target [H, P+1] complex.
-    precision "d", "f", or "mixed": float tracking to t_switch (with handover), then
-    double resumed from each path's last accepted point, as the tracker library does.
+    precision "d", "f", or "mixed": the mixed tracker (double state and residual, float linear
+    algebra) to t_switch (>= 1: to t = 1), then double resumed from each path's stopping point,
+    as the tracker library does.
     Returns a dict of numpy arrays (endpoints [H*paths, N], flags, counters).
     """
     kw = dict(hx=hx, ht=ht, p_start=p_start, p_target=p_target, nthreads=nthreads, max_steps=max_steps,
@@ -280,19 +284,16 @@ def track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precisi
         return _track(pb, start_sols, precision=precision, polish_iters=polish_iters, **kw)
     if not t_switch > 0:
         return _track(pb, start_sols, precision="d", polish_iters=polish_iters, **kw)
-    st = dict(REFERENCE_STEP)
-    st.update(step or {})
-    st["corr_tol2"] = max(st["corr_tol2"], MIXED_F32_TOL2)
-    first = _track(pb, start_sols, precision="f", polish_iters=0,
-                   handover=(min(t_switch, MIXED_MAX_SWITCH), MIXED_FAIL_LIMIT), **dict(kw, step=st))
+    first = _track(pb, start_sols, precision="m", polish_iters=0,
+                   handover=(t_switch if t_switch < 1 else 0.0, MIXED_FAIL_LIMIT, cond_limit), **kw)
     return _track(pb, start_sols, precision="d", polish_iters=polish_iters, resume=first, **kw)
 
 
 def _track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precision="d",
            polish_iters=0, nthreads=0, max_steps=None, max_corr=None, incr=None, step=None, handover=None,
            resume=None):
-    rt = np.float64 if precision == "d" else np.float32
-    fn = lib().orc_track_d if precision == "d" else lib().orc_track_f
+    rt = np.float32 if precision == "f" else np.float64
+    fn = {"d": lib().orc_track_d, "f": lib().orc_track_f, "m": lib().orc_track_m}[precision]
     start_sols = np.asarray(start_sols)
     paths = start_sols.shape[0]
     ss = _cx(start_sols, rt)
@@ -320,7 +321,9 @@ def _track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precis
                dt_end=np.zeros(n), resid=np.zeros(n))
     s = _prob_struct(pb, polish_iters, max_steps, max_corr, incr, step)
     if handover is not None:
-        s.t_handover, s.fail_limit = handover
+        s.t_handover, s.fail_limit = handover[:2]
+        if len(handover) > 2:
+            s.cond_limit = handover[2]
     if resume is not None:
         s.resume = 1
         ep[...] = resume["endpoints_raw"].astype(rt)

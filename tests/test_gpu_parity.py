@@ -2,7 +2,8 @@
 
 FP64 and FP32 modes follow the oracle's operation order, so endpoints, flags
 and step/iteration counters must be identical (compared as values).  Mixed
-precision (FP32 to t_switch with handover, then FP64) is compared the same way
+precision (the mixed tracker with FP32 linear algebra and an FP64 residual, then FP64 for the
+paths it hands over) is compared the same way
 with the oracle's two-phase run, and by recall of the FP64 real endpoints.
 """
 import os
@@ -158,16 +159,33 @@ def test_mixed_bit_exact_vs_oracle(name, robust, t_switch):
 
 
 def test_mixed_handover_happens():
-    """The FP32 phase stops every path by t_switch, and the FP64 phase carries its step
+    """The mixed phase stops every path by t_switch, and the FP64 phase carries its step
     counts on (a path's steps are those of both phases, under one step cap)."""
     pb, ob, tg = inputs("generalized_3views_4pts")
     ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_MIXED, t_switch=0.5, max_steps=6)
     r_mixed = O.track(ob, ob.start_sols, precision="mixed", t_switch=0.5, max_steps=6, nthreads=NCPU, **oargs)
     compare(ws, r_mixed)
-    first = O._track(ob, ob.start_sols.astype(np.complex64), precision="f", max_steps=6, handover=(0.5, 3),
-                     hx=oargs["hx"].astype(np.complex64), ht=oargs["ht"].astype(np.complex64))
+    first = O._track(ob, ob.start_sols, precision="m", max_steps=6, handover=(0.5, O.MIXED_FAIL_LIMIT,
+                                                                               O.MIXED_COND_LIMIT), **oargs)
     assert (first["t_end"] <= 0.5 + 1e-6).all()
     assert (ws.steps.cpu().numpy() >= first["steps"]).all()
+
+
+@pytest.mark.parametrize("name,cond_limit", [("generalized_3views_4pts", 1e3), ("generalized_3views_4pts", 1e5),
+                                             ("uncalibrated_trifocal_rel_pos_CY", 1e4),
+                                             ("trifocal_2op1p_30x30", 1e4)])
+def test_mixed_conditioning_handover_bit_exact(name, cond_limit):
+    """The mixed tracker to t = 1 under the path-jump-free control, handing a path to FP64 after a
+    step whose FP32 solve had a pivot-magnitude span above cond_limit: both phases equal the
+    oracle's bit for bit, and some paths do take the FP64 phase."""
+    pb, ob, tg = inputs(name, n_hyp=2, seed=7)
+    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=2, cond_limit=cond_limit, **ROBUST)
+    r = O.track(ob, ob.start_sols, precision="mixed", polish_iters=2, nthreads=NCPU, cond_limit=cond_limit,
+                step=O.ROBUST_STEP, max_corr=3, max_steps=2000, **oargs)
+    compare(ws, r)
+    first = O._track(ob, ob.start_sols, precision="m", handover=(0.0, O.MIXED_FAIL_LIMIT, cond_limit),
+                     step=O.ROBUST_STEP, max_corr=3, max_steps=2000, nthreads=NCPU, **oargs)
+    assert 0 < (first["conv"] == 0).sum() < first["conv"].size
 
 
 @pytest.mark.parametrize("name", ["P3P", "generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY"])
@@ -205,13 +223,14 @@ def real_targets(ob, n_hyp, seed):
 @pytest.mark.parametrize("name", ["generalized_3views_4pts", "5pt_rel_pos_alg_form_quat",
                                   "uncalibrated_trifocal_rel_pos_CY"])
 def test_mixed_precision_recall(name):
-    """FP32 tracking to t = 0.9 then FP64, both runs with path-jump-free step control:
+    """The mixed tracker (FP32 linear algebra, FP64 residual) to t = 1, FP64 for the paths it hands
+    over, both runs with path-jump-free step control:
     >= 99.5% of the FP64 run's real endpoints are found by the mixed run within 1e-8
     (8 hypotheses: several hundred real endpoints, so that the bar admits a miss)."""
     pb, ob = ghc.Problem(name), O.Problem(name)
     tg = real_targets(ob, 8, 9)
     w64, _ = run_gpu(pb, ob, tg, ghc.PREC_FP64, polish=3, **ROBUST)
-    wmx, _ = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=3, t_switch=0.9, **ROBUST)
+    wmx, _ = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=3, **ROBUST)
     e64, emx = to_cx(w64.endpoints), to_cx(wmx.endpoints)
     c64, cmx = w64.conv.cpu().numpy() == 1, wmx.conv.cpu().numpy() == 1
     r64 = w64.resid.cpu().numpy()

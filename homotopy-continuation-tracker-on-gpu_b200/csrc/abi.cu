@@ -48,6 +48,10 @@ int track_code(int rc) {
     set_error("mixed precision needs d_steps, d_corr, d_t_end and d_dt_end (the FP32 -> FP64 handover state)");
     return GHC_ERR_ARG;
   }
+  if (rc == -24) {
+    set_error("the problem's tables and coefficient buffers exceed one CTA's shared memory even at 32 threads");
+    return GHC_ERR_LIMIT;
+  }
   return cuda_fail("tracker launch");
 }
 

@@ -319,11 +319,12 @@ int load_problem(const std::string& root, const std::string& name, Problem& pb) 
       set_error("cannot read " + f);
       return GHC_ERR_IO;
     }
-    if (n < pb.P) {
-      set_error(f + ": fewer parameters than Num_Of_Params");
-      return GHC_ERR_FORMAT;
-    }
-    std::copy(v.begin(), v.begin() + 2 * pb.P, dst.begin());
+    // The reference reads as many pairs as the file holds (Data_Reader.cpp:140-149, 166-175) and
+    // leaves the rest of its parameter array unset; uncalibrated_trifocal_rel_pos_CH ships 18 of
+    // its 24 target parameters.  Missing trailing parameters are 0 here (deterministic), extra
+    // pairs beyond Num_Of_Params are ignored.
+    const long use = std::min<long>(n, pb.P);
+    std::copy(v.begin(), v.begin() + 2 * use, dst.begin());
     dst[2 * pb.P] = 1.0;
     dst[2 * pb.P + 1] = 0.0;
   }

@@ -12,15 +12,34 @@ namespace launch_detail {
 
 constexpr int kBlock = 128;
 
+// Threads per CTA: 128, or fewer (64, 32) when that many sub-warps' shared memory (per-sub-warp
+// coefficient buffers grow with the problem's coefficient count: 565 complex values x 2 for the
+// generalized 3-view 6-line problem) exceeds what one CTA may use.  0: does not fit at all.
+inline int block_threads(size_t tables, size_t per_sub, int W) {
+  static int optin = 0;
+  if (optin == 0) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || v <= 0) v = 48 * 1024;
+    optin = v;
+  }
+  for (int b = kBlock; b >= 32; b /= 2)
+    if (tables + (size_t)(b / W) * per_sub <= (size_t)optin) return b;
+  return 0;
+}
+
 template <typename R, typename RL, int N, int KIND, int V, int S>
 int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
   constexpr int W = (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
   auto kern = dev::track_kernel<R, RL, N, W, KIND, V, S>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
-  const int subs = kBlock / W;
   const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
-  const size_t smem = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) +
-                      subs * dev::sub_bytes(N, Mc, W, slots, 2 * (int)sizeof(RL), 2 * (int)sizeof(R));
+  const size_t tables = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms);
+  const size_t per_sub = dev::sub_bytes(N, Mc, W, slots, 2 * (int)sizeof(RL), 2 * (int)sizeof(R));
+  const int block = block_threads(tables, per_sub, W);
+  if (block == 0) return -24;
+  const int subs = block / W;
+  const size_t smem = tables + subs * per_sub;
   // Host calls in the launch path delay small launches, so per instantiation and device the
   // shared-memory attribute is only ever raised (to the largest size asked for, so a concurrent
   // launch never sees it below its own size) and the occupancy of the last size is kept.
@@ -37,17 +56,18 @@ int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
     if (e != cudaSuccess) return -20;
     if (attr_max[d].compare_exchange_weak(have, (long long)smem)) break;
   }
-  int occ = occ_key[d].load() == (long long)smem + 1 ? occ_val[d].load() : 0;
+  const long long okey = (long long)smem * 256 + block + 1;
+  int occ = occ_key[d].load() == okey ? occ_val[d].load() : 0;
   if (occ < 1) {
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBlock, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, block, smem);
     if (e != cudaSuccess || occ < 1) return -21;
     occ_val[d].store(occ);
-    occ_key[d].store((long long)smem + 1);
+    occ_key[d].store(okey);
   }
   // persistent grid: fill the GPU once, but never launch more sub-warps than items; a launch
   // with fewer paths than one warp per scheduler of every SM gives each path its own warp
   TrackParams q = p;
-  const int warps = kBlock / 32;
+  const int warps = block / 32;
   q.spread = (W < 32 && p.n_items <= (long long)n_sm * warps) ? 1 : 0;
   const int per_cta = q.spread ? warps : subs;
   long long grid = (long long)occ * n_sm;
@@ -60,7 +80,7 @@ int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
     e = cudaMemsetAsync(p.counter, 0, sizeof(int), s);
     if (e != cudaSuccess) return -22;
   }
-  kern<<<(unsigned)grid, kBlock, smem, s>>>(q);
+  kern<<<(unsigned)grid, block, smem, s>>>(q);
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : -23;
 }
@@ -82,15 +102,18 @@ int launch_polish_s(const PolishParams& p, cudaStream_t s) {
   constexpr int W = (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
   auto kern = dev::polish_kernel<N, W, KIND, S>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
-  const int subs = kBlock / W;
   const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
-  const size_t smem =
-      dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms) + subs * dev::sub_bytes(N, Mc, W, slots, 16, 16);
+  const size_t tables = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms);
+  const size_t per_sub = dev::sub_bytes(N, Mc, W, slots, 16, 16);
+  const int block = block_threads(tables, per_sub, W);
+  if (block == 0) return -24;
+  const int subs = block / W;
+  const size_t smem = tables + subs * per_sub;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -20;
   long long grid = (p.n_items + subs - 1) / subs;
   if (grid > 65535LL * 16) grid = 65535LL * 16;
   if (grid < 1) grid = 1;
-  kern<<<(unsigned)grid, kBlock, smem, s>>>(p);
+  kern<<<(unsigned)grid, block, smem, s>>>(p);
   return cudaGetLastError() == cudaSuccess ? 0 : -23;
 }
 

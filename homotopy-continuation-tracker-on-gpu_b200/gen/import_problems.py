@@ -6,8 +6,8 @@ dHdx_indx.txt, dHdt_indx.txt) into ``problems/<p>/`` and, for P2C problems,
 derives ``p2c_terms.txt`` from the problem's ``sys_<p>.m`` with p2c_gen.derive
 (which also checks both shipped tables against the polynomial system).
 
-usage: python import_problems.py [GPU-HC-checkout-root] [problem ...]
-The default root is the reference tree mounted next to this build.
+usage: python import_problems.py <GPU-HC-checkout-root> [problem ...]
+(the root may also come from the GHC_REFERENCE_ROOT environment variable).
 """
 import os
 import shutil
@@ -31,6 +31,17 @@ DEFAULT_PROBLEMS = [
     "dual_reciever_TDOA_5pt",
     "distorted_2view_triangulation",
     "P3P_10x10",
+    "3pt_rel_pos_homog",
+    "4view_triangulation",
+    "5pt_rel_pos_full_form_quat",
+    "5pt_rel_pos_geo_form_quat",
+    "6pt_RS_abs_pos_1lin",
+    "PnP_unkn_principal_pt",
+    "generalized_3views_6lines",
+    "optimal_P4P_abs_pos",
+    "optimal_PnP_quat",
+    "rel_pos_quiver",
+    "uncalibrated_trifocal_rel_pos_CH",
 ]
 
 FILES = ["gpuhc_settings.yaml", "start_params.txt", "target_params.txt", "start_sols.txt",
@@ -57,7 +68,9 @@ def import_problem(root, name):
 
 
 def main(argv):
-    root = argv[1] if len(argv) > 1 else "/root/reference"
+    root = argv[1] if len(argv) > 1 else os.environ.get("GHC_REFERENCE_ROOT")
+    if not root:
+        sys.exit(__doc__)
     names = argv[2:] or DEFAULT_PROBLEMS
     for n in names:
         try:

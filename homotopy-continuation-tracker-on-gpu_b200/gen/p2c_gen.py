@@ -14,8 +14,8 @@ Two modes:
   reference layout plus ``p2c_terms.txt``.
 
 ``p2c_terms.txt`` lists c_k(p) = sum_terms (num/den) * prod_j p_j and is what
-the product's coefficient builder (csrc/p2c.cpp, csrc/p2c_kernel.cu) expands
-into the per-hypothesis tables c_k(t) = c_k(q + t (p - q)).
+the product's coefficient builders (host: csrc/problem.cpp p2c_host, device:
+csrc/p2c.cu) expand into the per-hypothesis tables c_k(t) = c_k(q + t (p - q)).
 
 Table layout (reference, GPU-HC/magmaHC/gpu-idx-evals/dev-eval-indxing-P3P.cuh:69-120):
   dHdx[row][col][term][part], part = [scale, k, var_0 .. var_{Px-3}]
@@ -121,6 +121,11 @@ def derive(problem_dir, sys_m_path):
     Tx, Px = int(y["dHdx_Max_Terms"]), int(y["dHdx_Max_Parts"])
     Tt, Pt = int(y["dHdt_Max_Terms"]), int(y["dHdt_Max_Parts"])
     xs, ps, eqs = parse_matlab_system(sys_m_path)
+    # a system may declare trailing parameters its equations never use (optimal_PnP_quat declares
+    # p1..p85 and uses p1..p81, as its YAML's Num_Of_Params says): drop those
+    used = set().union(*[e.free_symbols for e in eqs]) if eqs else set()
+    while len(ps) > P and ps[-1] not in used:
+        ps = ps[:-1]
     if len(xs) != N or len(ps) != P or len(eqs) != N:
         raise ValueError("system %s: %d vars %d params %d eqs, yaml says N=%d P=%d"
                          % (sys_m_path, len(xs), len(ps), len(eqs), N, P))

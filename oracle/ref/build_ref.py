@@ -77,7 +77,18 @@ extern "C" void ref_eval_%(name)s(const double* x, const double* c, const double
   }
 }
 """
-DEFAULT_ROOT = "/root/reference"
+def reference_root():
+    """The reference checkout: $GHC_REFERENCE_ROOT, else a checkout named "reference" beside this
+    repository; None when neither holds GPU-HC/ (the GPU box has no reference tree)."""
+    for root in (os.environ.get("GHC_REFERENCE_ROOT"),
+                 os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
+                              "..", "reference")):
+        if root and os.path.isdir(os.path.join(root, "GPU-HC")):
+            return os.path.normpath(root)
+    return None
+
+
+DEFAULT_ROOT = reference_root()
 
 WRAP_HEAD = """// generated by oracle/ref/build_ref.py -- wrappers around the reference P2C builders
 #include <cstddef>
@@ -101,6 +112,17 @@ struct Buf {
   static void load(const REF_REAL* s, ref_cx* d, int n) { for (int i = 0; i < n; ++i) d[i] = ref_cx(s[2*i], s[2*i+1]); }
   static void store(const ref_cx* s, REF_REAL* d, int n) { for (int i = 0; i < n; ++i) { d[2*i] = s[i].x; d[2*i+1] = s[i].y; } }
 };
+}
+"""
+
+WRAP_NUM_FN = """extern "C" void ref_p2c_%(name)s_%(tag)s(const REF_REAL* tgt, const REF_REAL* st, REF_REAL* hx, REF_REAL* ht) {
+  // this problem's reference builder is numerical: the tables of its shipped parameters only
+  static const int NP = 4096;
+  ref_cx HX[NP], HT[NP];
+  (void)tgt;
+  (void)st;
+  ref_%(tag)s::magmaHCWrapper::p2c_numerical_%(name)s(HX, HT);
+  Buf<0>::store(HX, hx, %(nhx)d); Buf<0>::store(HT, ht, %(nht)d);
 }
 """
 
@@ -128,21 +150,26 @@ PKG_PROBLEMS = os.path.join(os.path.dirname(ORACLE), "homotopy-continuation-trac
 
 
 def problems_with_p2c(root):
-    """P2C problems of the reference that this package imports."""
+    """P2C problems of the reference that this package imports: (name, builder header, P, M, K,
+    numeric), numeric when the reference's builder is a fixed table of the shipped parameters
+    (p2c-numerical_<name>.h)."""
     wanted = set(os.listdir(PKG_PROBLEMS)) if os.path.isdir(PKG_PROBLEMS) else None
     out = []
     for hdr in sorted(glob.glob(os.path.join(root, "GPU-HC/magmaHC/PHC_Coeffs/p2c-*.h"))):
         name = os.path.basename(hdr)[4:-2]
+        numeric = name.startswith("numerical_")
+        if numeric:
+            name = name[len("numerical_"):]
         if wanted is not None and name not in wanted:
             continue
         ydir = os.path.join(root, "GPU-HC/problems", name)
         if not os.path.isdir(ydir):
-            continue  # the numeric-only 6-lines builder has no same-named problem folder
+            continue
         y = _yaml(os.path.join(ydir, "gpuhc_settings.yaml"))
         if y.get("GPUHC_Type") != "P2C":
             continue
         P, M, K = int(y["Num_Of_Params"]), int(y["Num_Of_Coeffs_From_Params"]), int(y["Max_Order_Of_T"])
-        out.append((name, hdr, P, M, K))
+        out.append((name, hdr, P, M, K, numeric))
     return out
 
 
@@ -174,7 +201,7 @@ def build_eval(root=DEFAULT_ROOT, force=False, verbose=False):
         return None
     os.makedirs(OUT, exist_ok=True)
     probs = []
-    for name, _, P, M, K in problems_with_p2c(root):
+    for name, _, P, M, K, _ in problems_with_p2c(root):
         hdr = os.path.join(root, "GPU-HC/magmaHC/gpu-idx-evals/dev-eval-indxing-%s.cuh" % name)
         if not os.path.exists(hdr):
             continue
@@ -228,8 +255,9 @@ def build(root=DEFAULT_ROOT, force=False, verbose=False):
     for real, tag in (("double", "d"), ("float", "f")):
         includes = "\n".join('#include "%s"' % p[1] for p in probs)
         src = WRAP_HEAD % dict(real=real, tag=tag, includes=includes)
-        for name, _, P, M, K in probs:
-            src += WRAP_FN % dict(name=name, tag=tag, np=P + 1, nhx=(M + 1) * (K + 1), nht=(M + 1) * K)
+        for name, _, P, M, K, numeric in probs:
+            src += (WRAP_NUM_FN if numeric else WRAP_FN) % dict(name=name, tag=tag, np=P + 1, nhx=(M + 1) * (K + 1),
+                                                                nht=(M + 1) * K)
         cpp = os.path.join(OUT, "p2c_ref_%s.cpp" % tag)
         with open(cpp, "w") as f:
             f.write(src)
@@ -244,8 +272,8 @@ def build(root=DEFAULT_ROOT, force=False, verbose=False):
     subprocess.check_call(["g++", "-shared", "-o", tmp] + objs)
     os.replace(tmp, LIB)
     with open(os.path.join(OUT, "problems.txt"), "w") as f:
-        for name, _, P, M, K in probs:
-            f.write("%s %d %d %d\n" % (name, P, M, K))
+        for name, _, P, M, K, numeric in probs:
+            f.write("%s %d %d %d %d\n" % (name, P, M, K, numeric))
     return LIB
 
 

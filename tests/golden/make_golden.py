@@ -14,7 +14,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GHC_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout> (or set GHC_REFERENCE_ROOT)")
     shutil.copyfile(os.path.join(root, "GPU-HC", "Output_Write_Files", "GPU_Converged_HC_tracks.txt"),
                     os.path.join(HERE, "cy_golden_tracks.txt"))
     print("wrote", os.path.join(HERE, "cy_golden_tracks.txt"))

@@ -21,7 +21,8 @@ sys.path.insert(0, GEN)
 import make_p3p_td  # noqa: E402
 import p2c_gen  # noqa: E402
 
-REF = "/root/reference"
+REF = os.environ.get("GHC_REFERENCE_ROOT") or os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(
+    os.path.abspath(__file__)))), "reference")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")

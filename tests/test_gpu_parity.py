@@ -19,7 +19,10 @@ pytestmark = pytest.mark.gpu
 
 SUPPORTED = ["P3P", "5pt_rel_pos_alg_form_quat", "generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY",
              "3view_triangulation", "6pt_RS_abs_pos", "dual_reciever_TDOA_5pt", "distorted_2view_triangulation",
-             "P3P_10x10", "trifocal_2op1p_30x30", "P3P_TD"]
+             "P3P_10x10", "trifocal_2op1p_30x30", "P3P_TD", "3pt_rel_pos_homog", "4view_triangulation",
+             "5pt_rel_pos_full_form_quat", "5pt_rel_pos_geo_form_quat", "6pt_RS_abs_pos_1lin",
+             "PnP_unkn_principal_pt", "generalized_3views_6lines", "optimal_P4P_abs_pos", "optimal_PnP_quat",
+             "rel_pos_quiver", "uncalibrated_trifocal_rel_pos_CH"]
 NCPU = os.cpu_count() or 1
 
 
@@ -102,7 +105,8 @@ def test_fp64_bit_exact_vs_oracle(name):
 
 
 @pytest.mark.parametrize("name", ["P3P", "generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY",
-                                  "trifocal_2op1p_30x30", "5pt_rel_pos_alg_form_quat"])
+                                  "trifocal_2op1p_30x30", "5pt_rel_pos_alg_form_quat", "generalized_3views_6lines",
+                                  "uncalibrated_trifocal_rel_pos_CH", "optimal_PnP_quat"])
 def test_fp32_bit_exact_vs_oracle(name):
     pb, ob, tg = inputs(name)
     ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_FP32)

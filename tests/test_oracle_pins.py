@@ -17,7 +17,15 @@ from lu_cases import SIZES, cases, strict_argmax
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "cy_golden_tracks.txt")
 P2C_PROBLEMS = ["P3P", "5pt_rel_pos_alg_form_quat", "generalized_3views_4pts", "uncalibrated_trifocal_rel_pos_CY",
                 "3view_triangulation", "6pt_RS_abs_pos", "dual_reciever_TDOA_5pt", "distorted_2view_triangulation",
-                "P3P_10x10"]
+                "P3P_10x10", "3pt_rel_pos_homog", "4view_triangulation", "5pt_rel_pos_full_form_quat",
+                "5pt_rel_pos_geo_form_quat", "6pt_RS_abs_pos_1lin", "PnP_unkn_principal_pt", "generalized_3views_6lines",
+                "optimal_P4P_abs_pos", "optimal_PnP_quat", "rel_pos_quiver", "uncalibrated_trifocal_rel_pos_CH"]
+# the reference's coefficient builder of this problem is a fixed table
+# (GPU-HC/magmaHC/PHC_Coeffs/p2c-numerical_generalized_3views_6lines.h)
+NUMERIC_P2C = {"generalized_3views_6lines"}
+# reference builders (GPU-HC/magmaHC/PHC_Coeffs/p2c-<p>.h) that disagree with the problem's own
+# system sys_<p>.m: some c_k(0) differ, and the shipped start solutions solve the .m system only
+BUILDER_MISMATCH = {"6pt_RS_abs_pos_1lin", "optimal_P4P_abs_pos"}
 ALL_PROBLEMS = P2C_PROBLEMS + ["trifocal_2op1p_30x30"]
 
 
@@ -66,13 +74,51 @@ def test_golden_cy_run(prec):
 @pytest.mark.parametrize("name", P2C_PROBLEMS)
 def test_p2c_matches_reference_builder(name):
     pb = O.Problem(name)
+    if name in BUILDER_MISMATCH or name in NUMERIC_P2C:
+        pytest.skip("pinned by test_reference_builder_quirks")
     rng = np.random.default_rng(1)
-    for target in [pb.target_params, np.append(rng.normal(size=pb.P) + 1j * rng.normal(size=pb.P), 1.0)]:
+    targets = [pb.target_params, np.append(rng.normal(size=pb.P) + 1j * rng.normal(size=pb.P), 1.0)]
+    for target in targets:
         hx, ht = coefs(pb, target)
         rhx, rht = O.ref_p2c(pb, pb.start_params, target, "d")
         scale = max(1.0, np.abs(rhx).max())
         assert np.abs(hx - rhx).max() <= 1e-12 * scale
         assert np.abs(ht - rht).max() <= 1e-12 * max(1.0, np.abs(rht).max())
+
+
+def start_residual(pb, hx, ht):
+    worst = 0.0
+    for p in range(0, pb.paths, max(1, pb.paths // 40)):
+        H, _, _ = O.eval_system(pb, pb.start_sols[p], 0.0, hx=hx, ht=ht)
+        worst = max(worst, np.abs(H).max() / max(1.0, np.abs(pb.start_sols[p]).max() ** 2))
+    return worst
+
+
+@pytest.mark.skipif(not O.ref_p2c_available(), reason="oracle/_ref not built (needs the reference tree)")
+@pytest.mark.parametrize("name", sorted(BUILDER_MISMATCH | NUMERIC_P2C))
+def test_reference_builder_quirks(name):
+    """Where the reference's coefficient builder disagrees with its own problem data, the build
+    keeps the coefficients of the problem's system sys_<p>.m (whose start system the shipped start
+    solutions solve) and pins the disagreement:
+    * 6pt_RS_abs_pos_1lin, optimal_P4P_abs_pos: the builder's c_k(0) differ for some k, and the
+      shipped start solutions do not solve the builder's start system;
+    * generalized_3views_6lines: the builder is a fixed numerical table whose c_k(0) equal ours
+      (the start system agrees) but whose t-dependence encodes another target than the shipped
+      target_params.txt, and whose constant-1 sentinel c_M is 0."""
+    pb = O.Problem(name)
+    hx, ht = coefs(pb)
+    rhx, rht = O.ref_p2c(pb, pb.start_params, pb.target_params, "d")
+    K, M = pb.K, pb.M
+    assert start_residual(pb, hx, ht) < 1e-9
+    c0, r0 = hx.reshape(-1, K + 1)[:, 0], rhx.reshape(-1, K + 1)[:, 0]
+    if name in NUMERIC_P2C:
+        assert np.abs(c0[:M] - r0[:M]).max() <= 1e-12 * max(1.0, np.abs(r0).max())
+        assert c0[M] == 1 and r0[M] == 0
+        assert np.abs(hx - rhx).max() > 1.0
+    else:
+        assert start_residual(pb, rhx, rht) > 1.0
+        bad = np.abs(c0 - r0) > 1e-9 * max(1.0, np.abs(r0).max())
+        assert 0 < bad.sum() < M // 2
 
 
 @pytest.mark.parametrize("name", ALL_PROBLEMS)

@@ -22,7 +22,7 @@ namespace ghc {
 
 enum Kind : int { KIND_P2C = 0, KIND_PH = 1 };
 enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1, PREC_MIXED = 2 };
-enum Status : int { ST_CONVERGED = 0, ST_DIVERGED = 1, ST_STEP_CAP = 2 };
+enum Status : int { ST_CONVERGED = 0, ST_DIVERGED = 1, ST_STEP_CAP = 2, ST_NONFINITE = 3, ST_SINGULAR = 4 };
 
 constexpr int kMaxN = 32;
 constexpr int kMaxVarsPerTerm = 7;

@@ -383,8 +383,9 @@ __device__ __forceinline__ int pivot_exact(R m, bool cand, int pos, int i) {
   return mp;
 }
 
-// PivotRange: the span of the pivot magnitudes |U_ii| (|Re|+|Im|) of one solve and whether one was
-// NaN, the mixed tracker's conditioning test (computed by every solve; unused results cost nothing)
+// PivotRange: the span of the pivot magnitudes |U_ii| (|Re|+|Im|) of one solve (a NaN in column 0
+// stays, later NaNs are skipped, as in the oracle's comparisons) and whether one was NaN: the mixed
+// tracker's conditioning test, and lo == 0 marks a singular solve (a zero pivot)
 template <typename R>
 struct PivotRange {
   R lo, hi;
@@ -428,14 +429,9 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
       else if (pos == i) pos = bp;
     }
     const bool zero = (pm == R(0));
-    if (i == 0) {
-      rg.lo = rg.hi = pm;
-      rg.nan = pm != pm;
-    } else {
-      rg.lo = fmin(rg.lo, pm);
-      rg.hi = fmax(rg.hi, pm);
-      rg.nan = rg.nan || pm != pm;
-    }
+    rg.lo = (i == 0 || pm < rg.lo) ? pm : rg.lo;
+    rg.hi = (i == 0 || pm > rg.hi) ? pm : rg.hi;
+    rg.nan = (i != 0 && rg.nan) || pm != pm;
     // (a zero pivot's reciprocal is NaN, as the oracle's c_rcp(0))
     const cx<R> rc = c_rcp(p_i);
     // the pivot row's reciprocal waits in the solution slot of its position until the back
@@ -513,8 +509,8 @@ __device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, c
       else if (pos == i) pos = bp;
     }
     const bool zero = (pm == R(0));
-    rg.lo = i == 0 ? pm : fmin(rg.lo, pm);
-    rg.hi = i == 0 ? pm : fmax(rg.hi, pm);
+    rg.lo = (i == 0 || pm < rg.lo) ? pm : rg.lo;
+    rg.hi = (i == 0 || pm > rg.hi) ? pm : rg.hi;
     rg.nan = (i != 0 && rg.nan) || pm != pm;
     const cx<R> rc = c_rcp(zero ? mk(R(0), R(0)) : p_i);
     if (is_piv) myrcp = rc;
@@ -615,20 +611,21 @@ __device__ __forceinline__ void eval_any(const Tables& tb, const SubMem& sm, int
 // RL solve is too ill-conditioned to keep Newton's contraction
 template <typename R, typename RL, int N, int W, int KIND, int S>
 __device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, int l, int which, double cond_limit,
-                                            bool& ill) {
+                                            bool& ill, bool& sing) {
   cx<RL> A[N];
   cx<RL> b;
   eval_any<R, RL, N, W, KIND, S>(tb, sm, l, A, b, which);
   PivotRange<RL> rg;
   lu_solve<RL, N, W>(A, b, l, view<RL>(sm.sx), view<RL>(sm.sol), rg);
   ill = cond_limit > 0.0 && (rg.nan || !(rg.hi <= (RL)cond_limit * rg.lo));
+  sing = rg.lo == RL(0);
   const cx<RL> k = (l < N) ? view<RL>(sm.sol)[l] : mk(RL(0), RL(0));
   return c_cast<R>(k);
 }
 template <typename R, typename RL, int N, int W, int KIND, int S>
 __device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, int l, int which) {
-  bool ill;
-  return eval_solve<R, RL, N, W, KIND, S>(tb, sm, l, which, 0.0, ill);
+  bool ill, sing;
+  return eval_solve<R, RL, N, W, KIND, S>(tb, sm, l, which, 0.0, ill, sing);
 }
 
 // the track into shared memory: in RL for H_x and H_t, and (mixed) in R for the residual
@@ -838,6 +835,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
   R coef_t = R(-1);  // the t at which this sub-warp's coefficient buffers hold c_k(t) (-1: none)
   bool end_zone = false, success = false, inf = false, finished = false;
   bool step_ill = false, ill_stop = false;  // mixed: a solve of this step was ill-conditioned; stop after it
+  bool step_sing = false, last_sing = false;  // a solve of this step / the last completed step had a zero pivot
   int nsucc = 0, step = 0, ncorr = 0, phase = 0, cit = 0, nfail = 0;
   const R dt_init = (KIND == KIND_PH) ? R(0.01) : R(0.05);
 
@@ -858,6 +856,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
     phase = 0;
     cit = 0;
     step_ill = false;
+    step_sing = false;
   };
   // the path stops before its next step (kernel_HC_Solver_P3P.cu:247-249, plus the handover rules)
   auto at_end = [&]() -> bool {
@@ -890,7 +889,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
     inf = false;
     nsucc = 0;
     nfail = 0;
-    step_ill = ill_stop = false;
+    step_ill = ill_stop = step_sing = last_sing = false;
     finished = at_end();
     if (!finished) prologue();
   };
@@ -919,7 +918,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
     rec_i[4] = nfail;
     rec_i[5] = nsucc;
     rec_i[6] = (alive ? 1 : 0) | (finished ? 2 : 0) | (end_zone ? 4 : 0) | (success ? 8 : 0) | (inf ? 16 : 0) |
-               (step_ill ? 32 : 0) | (ill_stop ? 64 : 0);
+               (step_ill ? 32 : 0) | (ill_stop ? 64 : 0) | (step_sing ? 128 : 0) | (last_sing ? 256 : 0);
   };
   auto unstash = [&]() {
     t0 = rec_r[0];
@@ -944,6 +943,8 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
     inf = (f >> 4) & 1;
     step_ill = (f >> 5) & 1;
     ill_stop = (f >> 6) & 1;
+    step_sing = (f >> 7) & 1;
+    last_sing = (f >> 8) & 1;
     const volatile cx<R>* xv = reinterpret_cast<const volatile cx<R>*>(sm.xst);
     x = (l < N) ? mk(xv[l].re, xv[l].im) : mk(R(0), R(0));
   };
@@ -963,10 +964,11 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
     write_track<R, RL, N>(sm, l, x);
     stash();
     __syncwarp(kFull);
-    bool ill = false;
-    const cx<R> v = eval_solve<R, RL, N, W, KIND, S>(tb, sm, l, rk ? 1 : 0, p.cond_limit, ill);
+    bool ill = false, sing = false;
+    const cx<R> v = eval_solve<R, RL, N, W, KIND, S>(tb, sm, l, rk ? 1 : 0, p.cond_limit, ill, sing);
     unstash();
     if (served && ill) step_ill = true;
+    if (served && sing) step_sing = true;
     // ---------------- corrector norms (kernel_HC_Solver_P3P.cu:204-219), all lanes take part
     R ns0 = 0, nc0 = 0;
     if (__any_sync(kFull, corr)) {
@@ -1033,6 +1035,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
       }
       ++step;
       if (step_ill) ill_stop = true;
+      last_sing = step_sing;
       if (!done) done = at_end();
       if (done && !inf && p.t_handover > 0.0 && f_sub(t_hand, t0) <= R(1e-6) && step <= p.max_steps &&
           dt < dt_pre)
@@ -1041,6 +1044,9 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
     }
 
     // ---------------- finished paths: write out and take the next path
+    // (a non-finite track anywhere in the sub-warp; every lane takes part in the vote)
+    const unsigned bad = __ballot_sync(kFull, l < N && !(isfinite(x.re) && isfinite(x.im)));
+    const bool nonfinite = ((W == 32 ? bad : bad >> leader) & (W == 32 ? kFull : ((1u << (W & 31)) - 1u))) != 0u;
     if (done && primary) {
       R* ep = reinterpret_cast<R*>(p.endpoints) + 2 * item * p.ld_out;
       if (l < N) {
@@ -1051,7 +1057,12 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
         const bool conv = (t0 >= R(1) || f_sub(R(1), t0) <= R(1e-7));
         if (p.conv) p.conv[item] = conv ? 1 : 0;
         if (p.infy) p.infy[item] = inf ? 1 : 0;
-        if (p.status) p.status[item] = conv ? ST_CONVERGED : (inf ? ST_DIVERGED : ST_STEP_CAP);
+        if (p.status)
+          p.status[item] = conv        ? ST_CONVERGED
+                           : inf       ? ST_DIVERGED
+                           : nonfinite ? ST_NONFINITE
+                           : last_sing ? ST_SINGULAR
+                                       : ST_STEP_CAP;
         if (p.steps) p.steps[item] = step;
         if (p.corr) p.corr[item] = ncorr;
         // a path handed over at the boundary resumes at exactly t_handover, not at its float t

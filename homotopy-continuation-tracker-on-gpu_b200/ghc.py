@@ -21,7 +21,7 @@ PREC_FP64, PREC_FP32, PREC_MIXED = 0, 1, 2
 # first Newton update, bounded step.  Used with a corrector limit of 3.
 ROBUST_STEP = dict(corr_tol2=1e-12, first_tol2=1e-2, dt_max=0.05)
 KIND_P2C, KIND_PH = 0, 1
-STATUS_CONVERGED, STATUS_DIVERGED, STATUS_STEP_CAP = 0, 1, 2
+STATUS_CONVERGED, STATUS_DIVERGED, STATUS_STEP_CAP, STATUS_NONFINITE, STATUS_SINGULAR = 0, 1, 2, 3, 4
 
 if not os.path.exists(LIB_PATH):
     raise ImportError("libghc_b200.so is not built (run homotopy-continuation-tracker-on-gpu_b200/build.py)")

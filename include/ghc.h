@@ -39,6 +39,8 @@ extern "C" {
 #define GHC_STATUS_CONVERGED 0
 #define GHC_STATUS_DIVERGED 1 /* |x|^2 > 1e14 in the corrector ("infinity") */
 #define GHC_STATUS_STEP_CAP 2 /* ran out of steps before t = 1 */
+#define GHC_STATUS_NONFINITE 3 /* stopped with a NaN or infinite component in its track */
+#define GHC_STATUS_SINGULAR 4  /* stopped (step cap or handover) after a step in which a solve had a zero pivot */
 
 typedef struct ghc_problem ghc_problem;
 

@@ -23,7 +23,7 @@
 #define ORC_MMAX 640
 
 enum { ORC_P2C = 0, ORC_PH = 1 };
-enum { ORC_CONVERGED = 0, ORC_DIVERGED = 1, ORC_STEP_CAP = 2 };
+enum { ORC_CONVERGED = 0, ORC_DIVERGED = 1, ORC_STEP_CAP = 2, ORC_NONFINITE = 3, ORC_SINGULAR = 4 };
 
 /* Problem description: the YAML sizes plus the raw index tables in the
  * reference layout (GPU-HC/magmaHC/GPU_HC_Solver.cpp:44-83). */

@@ -281,7 +281,8 @@ static void SFX(lu_solve_trace)(int N, CX A[][ORC_NMAX], CX* b, CX* z, int32_t* 
 static void SFX(lu_solve)(int N, CX A[][ORC_NMAX], CX* b, CX* z) { SFX(lu_solve_trace)(N, A, b, z, NULL, NULL, NULL); }
 
 /* one evaluation + solve: z = H_x^{-1} * rhs; rhs = -H_t (which=1) or H (which=0) */
-static void SFX(eval_solve)(const orc_problem* pb, const COEFS* cf, const CX* x, int which, CX* z, int* ill) {
+static void SFX(eval_solve)(const orc_problem* pb, const COEFS* cf, const CX* x, int which, CX* z, int* ill,
+                            int* sing) {
   const int N = pb->N;
   (void)ill;
 #ifdef ORC_MIXED_LA
@@ -303,6 +304,7 @@ static void SFX(eval_solve)(const orc_problem* pb, const COEFS* cf, const CX* x,
     }
     float range[3] = {0, 0, 0};
     lu_solve_trace_f(N, A, b, zf, NULL, NULL, range);
+    if (sing && range[0] == 0) *sing = 1;
     for (int r = 0; r < N; ++r) z[r] = SFX(c_make)((double)zf[r].re, (double)zf[r].im);
     /* ill-conditioned for the float solve: the pivot magnitudes span more than cond_limit (or NaN) */
     if (pb->cond_limit > 0 && ill && (range[2] != 0 || !(range[1] <= (float)pb->cond_limit * range[0]))) *ill = 1;
@@ -316,7 +318,9 @@ static void SFX(eval_solve)(const orc_problem* pb, const COEFS* cf, const CX* x,
     CX h = SFX(eval_h_row)(pb, cf, x, r, which);
     b[r] = which ? SFX(c_make)(-h.re, -h.im) : h;
   }
-  SFX(lu_solve)(N, A, b, z);
+  REAL range[3] = {0, 0, 0};
+  SFX(lu_solve_trace)(N, A, b, z, NULL, NULL, range);
+  if (sing && range[0] == 0) *sing = 1;
 }
 
 /*
@@ -352,6 +356,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
 
   REAL dt_pre = dt; /* the step without the handover clamp: the next phase resumes with it */
   int ill = 0, ill_stop = 0; /* mixed: a solve of this step was ill-conditioned for float; stop after it */
+  int step_sing = 0, last_sing = 0; /* a solve of this step / of the last completed step had a zero pivot */
   for (int step = steps; step <= pb->max_steps; ++step) {
     if (!(t0 < (REAL)1 && (REAL)1 - t0 > (REAL)1e-7)) break;
     if (pb->t_handover > 0 && t_hand - t0 <= (REAL)1e-6) {
@@ -362,6 +367,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
     if (ill_stop) break;
     ++steps;
     ill = 0;
+    step_sing = 0;
     /* end-zone step clamp (kernel_HC_Solver_P3P.cu:121-131; PH edge 0.95 at trifocal_2op1p_30x30.cu:163-182) */
     if (!end_zone && FABS((REAL)1 - t0) <= (REAL)0.0500001) end_zone = 1;
     if (end_zone) {
@@ -378,7 +384,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
     /* loopy RK4 predictor (kernel_HC_Solver_P3P.cu:139-183) */
     for (int rk = 0; rk < 4; ++rk) {
       SFX(eval_coefs)(h, t0, cf);
-      SFX(eval_solve)(pb, cf, x, 1, k, &ill);
+      SFX(eval_solve)(pb, cf, x, 1, k, &ill, &step_sing);
       if (rk < 3) {
         const REAL a = dt * wgt[rk];
         const REAL d = dt * frac[rk];
@@ -402,7 +408,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
     inf = 0;
     for (int it = 0; it < pb->max_corr; ++it) {
       ++corr;
-      SFX(eval_solve)(pb, cf, x, 0, k, &ill);
+      SFX(eval_solve)(pb, cf, x, 0, k, &ill, &step_sing);
       REAL ns[ORC_NMAX], nc[ORC_NMAX];
       for (int r = 0; r < N; ++r) {
         x[r] = SFX(c_sub)(x[r], k[r]);
@@ -441,12 +447,19 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
       }
     }
     if (ill) ill_stop = 1;
+    last_sing = step_sing;
   }
 
   const int conv = (t0 >= (REAL)1 || ((REAL)1 - t0 <= (REAL)1e-7));
   out->converged = (uint8_t)conv;
   out->infinity = (uint8_t)inf;
-  out->status = conv ? ORC_CONVERGED : (inf ? ORC_DIVERGED : ORC_STEP_CAP);
+  int nonfinite = 0;
+  for (int r = 0; r < N; ++r) nonfinite |= !(isfinite(x[r].re) && isfinite(x[r].im));
+  out->status = conv ? ORC_CONVERGED
+                : inf ? ORC_DIVERGED
+                : nonfinite ? ORC_NONFINITE
+                : last_sing ? ORC_SINGULAR
+                : ORC_STEP_CAP;
   out->steps = steps;
   out->corr = corr;
   /* handed over at the boundary: resume at exactly t_handover (the tracker library does the same) */
@@ -458,7 +471,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
   if (conv) {
     SFX(eval_coefs)(h, (REAL)1, cf);
     for (int it = 0; it < pb->polish_iters; ++it) {
-      SFX(eval_solve)(pb, cf, x, 0, k, NULL);
+      SFX(eval_solve)(pb, cf, x, 0, k, NULL, NULL);
       for (int r = 0; r < N; ++r) x[r] = SFX(c_sub)(x[r], k[r]);
     }
     REAL hr[ORC_NMAX];

@@ -25,7 +25,7 @@ REPO = os.path.dirname(HERE)
 PKG_PROBLEMS = os.path.join(REPO, "homotopy-continuation-tracker-on-gpu_b200", "problems")
 
 P2C, PH = 0, 1
-CONVERGED, DIVERGED, STEP_CAP = 0, 1, 2
+CONVERGED, DIVERGED, STEP_CAP, NONFINITE, SINGULAR = 0, 1, 2, 3, 4
 
 # Evaluations tolerances (GPU-HC/magmaHC/definitions.hpp:24-26)
 DUPLICATE_SOL_DIFF_TOL = 1e-4

@@ -274,6 +274,27 @@ def test_scene_targets_bit_exact_vs_oracle(name, step):
     assert np.array_equal(ws.resid.cpu().numpy()[conv], r["resid"][conv])
 
 
+def test_path_status_singular_and_nonfinite():
+    """Per-path status beyond converged / diverged / step cap: a path started where H_x is singular
+    (x = 0 of the total-degree start system x_i^2 - 1, so every solve has a zero pivot) ends at the
+    step cap with its last solve singular, a path started at NaN ends non-finite; the others
+    converge.  Equal to the oracle's statuses."""
+    pb, ob, tg = inputs("P3P_TD")
+    starts = np.array(ob.start_sols)
+    starts[0] = 0.0
+    starts[1] = np.nan
+    hx = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[0] for t in tg])
+    ht = np.array([O.p2c_tables(ob.terms, ob.start_params, t)[1] for t in tg])
+    ws = ghc.Workspace(pb, 1, ghc.PREC_FP64)
+    ghc.track(pb, ws, cx_t(starts), d_coef_hx=cx_t(hx), d_coef_ht=cx_t(ht), max_steps=40)
+    torch.cuda.synchronize()
+    r = O.track(ob, starts, hx=hx, ht=ht, nthreads=NCPU, max_steps=40)
+    st = ws.status.cpu().numpy()
+    assert np.array_equal(st, r["status"])
+    assert st[0] == ghc.STATUS_SINGULAR and st[1] == ghc.STATUS_NONFINITE
+    assert (st[2:] == ghc.STATUS_CONVERGED).all()
+
+
 def test_step_cap_and_short_corrector():
     pb, ob, tg = inputs("generalized_3views_4pts")
     ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_FP64, max_steps=5, max_corr=2)

@@ -143,7 +143,7 @@ class Problem:
                 setattr(self, f, getattr(info, f))
         self.name = info.name.decode()
 
-    def device(self):
+    def bound_device(self):
         """Device holding the handle's compiled tables (uploaded by its first tracking call), -1: none."""
         info = ProblemInfo()
         _check(ghc_problem_get_info(self.h, ctypes.byref(info)), "ghc_problem_get_info")

@@ -164,16 +164,19 @@ int ghc_track(const ghc_problem* pb, const ghc_track_args* args, void* stream);
 /* ghc_track for callers that must not allocate device memory -- no counterpart
  * in the reference.  For applications that own all device memory through their
  * own pool or budget, or loops that cannot take cudaMalloc's synchronisation or
- * its failure mid-run.  Same arguments and results as ghc_track, except that
- * args->d_counter is ignored: the work-stealing counter and the compiled index
- * tables live in a fixed static device array of 64 KiB per device, held by
- * every GPU that loads the library until the process exits.  Problems whose
- * compiled tables do not fit return GHC_ERR_LIMIT.  The first call on each
- * device looks up the array's address (make it before any stream capture).
- * All calls on a device share the array and it keeps the last call's contents;
- * each call copies its tables in and clears the counter on `stream`, so calls
- * ordered on one stream are independent, while calls that overlap on the GPU
- * race.  Allocates nothing: no cudaMalloc, cudaFree or allocating library call. */
+ * its failure mid-run.  Same arguments and results as ghc_track (every precision
+ * mode, polish included), except that args->d_counter is ignored: the
+ * work-stealing counter and the compiled index tables live in a fixed static
+ * device array of 64 KiB per device, held by every GPU that loads the library
+ * until the process exits, and the problem handle itself stays without device
+ * memory.  Problems whose compiled tables do not fit return GHC_ERR_LIMIT.  The
+ * first call on each device looks up the array's address (make it before any
+ * stream capture).  All calls on a device share the array and it keeps the last
+ * call's contents: a call copies its tables in on `stream` unless the array
+ * already holds this handle's tables, and clears the counter on `stream`, so
+ * calls ordered on one stream are independent, while calls that overlap on the
+ * GPU race.  Allocates nothing: no cudaMalloc, cudaFree or allocating library
+ * call. */
 int ghc_track_noalloc(const ghc_problem* pb, const ghc_track_args* args, void* stream);
 
 /* ---------------------------------------------------------------------------

@@ -181,3 +181,35 @@ def test_tuning_setters_validate():
     for bad in [(ghc.PREC_FP64, 2, 0), (ghc.PREC_FP64, 0, 3), (ghc.PREC_FP64, 0, -2), (7, 0, 0)]:
         with pytest.raises(ghc.GhcError):
             ghc.set_tuning(pb, *bad)
+
+
+def test_no_alloc_rejects_tables_beyond_its_fixed_array(tmp_path):
+    """ghc_track_noalloc keeps the compiled tables in a fixed 64 KiB device array: a problem whose
+    tables need more is rejected with GHC_ERR_LIMIT (-8) and a message naming the sizes, before any
+    device work (the pointers below are never used) and without binding the handle to a device."""
+    import ctypes
+    N, Tx, Px, Tt, Pt, M, P, paths = 18, 30, 3, 1, 4, 40, 40, 2
+    d = tmp_path / "DENSE_18"
+    d.mkdir()
+    (d / "gpuhc_settings.yaml").write_text(
+        "problem_name: DENSE_18\nGPUHC_Type: P2C\nGPUHC_Max_Steps: 10\nGPUHC_Max_Correction_Steps: 3\n"
+        "GPUHC_Num_Of_Steps_to_Increase_Delta_t: 2\nNum_Of_Vars: %d\nNum_Of_Params: %d\nNum_Of_Tracks: %d\n"
+        "dHdx_Max_Terms: %d\ndHdx_Max_Parts: %d\ndHdt_Max_Terms: %d\ndHdt_Max_Parts: %d\nMax_Order_Of_T: 1\n"
+        "Num_Of_Coeffs_From_Params: %d\n" % (N, P, paths, Tx, Px, Tt, Pt, M))
+    pairs = "".join("%d 0\n" % (k + 1) for k in range(P))
+    (d / "start_params.txt").write_text(pairs)
+    (d / "target_params.txt").write_text(pairs)
+    (d / "start_sols.txt").write_text("1 0\n" * (N * paths))
+    hx = [[1, k % M, k % (N + 1)] for k in range(N * N * Tx)]   # every term a real (non-padding) term
+    (d / "dHdx_indx.txt").write_text("\n".join(" ".join(map(str, t)) for t in hx) + "\n")
+    ht = [[1, r % M, r % N, N] for r in range(N * Tt)]
+    (d / "dHdt_indx.txt").write_text("\n".join(" ".join(map(str, t)) for t in ht) + "\n")
+    pb = ghc.Problem("DENSE_18", root=str(tmp_path))
+    a = ghc.TrackArgs()
+    a.n_hyp, a.precision = 1, ghc.PREC_FP64
+    a.d_start_sols = a.d_endpoints = a.d_coef_hx = a.d_coef_ht = 256
+    rc = ghc.ghc_track_noalloc(pb.h, ctypes.byref(a), None)
+    assert rc == -8
+    msg = ghc.ghc_last_error().decode()
+    assert "65536" in msg and "ghc_track" in msg
+    assert pb.bound_device() == -1

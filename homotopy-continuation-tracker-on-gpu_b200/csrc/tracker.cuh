@@ -383,18 +383,34 @@ __device__ __forceinline__ int pivot_exact(R m, bool cand, int pos, int i) {
   return mp;
 }
 
-// PivotRange: the span of the pivot magnitudes |U_ii| (|Re|+|Im|) of one solve (a NaN in column 0
-// stays, later NaNs are skipped, as in the oracle's comparisons) and whether one was NaN: the mixed
-// tracker's conditioning test, and lo == 0 marks a singular solve (a zero pivot)
-template <typename R>
+// PivotRange: what one solve saw of its pivot magnitudes |U_ii| (|Re|+|Im|), in the oracle's
+// comparison order.  singular(): a zero pivot, unless column 0's magnitude was NaN (the oracle's
+// running minimum then stays NaN).  With SPAN (the mixed tracker's conditioning test) also the
+// smallest and largest magnitudes and whether any was NaN; without it only two flags stay live
+// across the LU.
+template <typename R, bool SPAN>
 struct PivotRange {
   R lo, hi;
-  bool nan;
+  bool nan, zero, nan0;
+  __device__ __forceinline__ void add(int i, R pm) {
+    if (i == 0) {
+      nan0 = pm != pm;
+      zero = pm == R(0);
+    } else {
+      zero = zero || pm == R(0);
+    }
+    if constexpr (SPAN) {
+      lo = (i == 0 || pm < lo) ? pm : lo;
+      hi = (i == 0 || pm > hi) ? pm : hi;
+      nan = (i != 0 && nan) || pm != pm;
+    }
+  }
+  __device__ __forceinline__ bool singular() const { return zero && !nan0; }
 };
 
-template <typename R, int N, int W>
+template <typename R, int N, int W, bool SPAN>
 __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
-                                                  PivotRange<R>& rg) {
+                                                  PivotRange<R, SPAN>& rg) {
   const bool live = l < N;
   int pos = l;
   static_for<0, N>([&](auto ic) {
@@ -429,9 +445,7 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
       else if (pos == i) pos = bp;
     }
     const bool zero = (pm == R(0));
-    rg.lo = (i == 0 || pm < rg.lo) ? pm : rg.lo;
-    rg.hi = (i == 0 || pm > rg.hi) ? pm : rg.hi;
-    rg.nan = (i != 0 && rg.nan) || pm != pm;
+    rg.add(i, pm);
     // (a zero pivot's reciprocal is NaN, as the oracle's c_rcp(0))
     const cx<R> rc = c_rcp(p_i);
     // the pivot row's reciprocal waits in the solution slot of its position until the back
@@ -467,9 +481,9 @@ __device__ __forceinline__ cx<R> pick(const cx<R> (&A)[N], int i) {
   return a;
 }
 
-template <typename R, int N, int W>
+template <typename R, int N, int W, bool SPAN>
 __device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
-                                                PivotRange<R>& rg) {
+                                                PivotRange<R, SPAN>& rg) {
   const bool live = l < N;
   int pos = l;
   cx<R> myrcp = mk(R(0), R(0));
@@ -509,9 +523,7 @@ __device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, c
       else if (pos == i) pos = bp;
     }
     const bool zero = (pm == R(0));
-    rg.lo = (i == 0 || pm < rg.lo) ? pm : rg.lo;
-    rg.hi = (i == 0 || pm > rg.hi) ? pm : rg.hi;
-    rg.nan = (i != 0 && rg.nan) || pm != pm;
+    rg.add(i, pm);
     const cx<R> rc = c_rcp(zero ? mk(R(0), R(0)) : p_i);
     if (is_piv) myrcp = rc;
     if (live && pos > i && !zero) {
@@ -535,14 +547,15 @@ __device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, c
   __syncwarp(kFull);
 }
 
-template <typename R, int N, int W>
-__device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol, PivotRange<R>& rg) {
+template <typename R, int N, int W, bool SPAN>
+__device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
+                                         PivotRange<R, SPAN>& rg) {
   if constexpr (kLuForm<N> == LU_ROLLED) lu_solve_rolled<R, N, W>(A, b, l, sx, sol, rg);
   else lu_solve_unrolled<R, N, W>(A, b, l, sx, sol, rg);
 }
 template <typename R, int N, int W>
 __device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
-  PivotRange<R> rg;
+  PivotRange<R, false> rg;
   lu_solve<R, N, W>(A, b, l, sx, sol, rg);
 }
 
@@ -615,10 +628,12 @@ __device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, 
   cx<RL> A[N];
   cx<RL> b;
   eval_any<R, RL, N, W, KIND, S>(tb, sm, l, A, b, which);
-  PivotRange<RL> rg;
+  constexpr bool kSpan = !std::is_same<R, RL>::value;  // only the mixed tracker tests conditioning
+  PivotRange<RL, kSpan> rg;
   lu_solve<RL, N, W>(A, b, l, view<RL>(sm.sx), view<RL>(sm.sol), rg);
-  ill = cond_limit > 0.0 && (rg.nan || !(rg.hi <= (RL)cond_limit * rg.lo));
-  sing = rg.lo == RL(0);
+  if constexpr (kSpan) ill = cond_limit > 0.0 && (rg.nan || !(rg.hi <= (RL)cond_limit * rg.lo));
+  else ill = false;
+  sing = rg.singular();
   const cx<RL> k = (l < N) ? view<RL>(sm.sol)[l] : mk(RL(0), RL(0));
   return c_cast<R>(k);
 }
@@ -791,7 +806,10 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 #else
 #define GHC_MINB(N, R, RL, V) track_min_blocks<N, R, RL, V>()
 #endif
-template <typename R, typename RL, int N, int W, int KIND, int V, int S>
+// WK >= 0: the H_x walk is fixed at compile time (only that walk's code is in the kernel, which
+// spares the register allocator the other walk's read-back: above 16 unknowns, where the row fills
+// most of the registers); WK < 0: chosen at run time from p.flat_eval.
+template <typename R, typename RL, int N, int W, int KIND, int V, int S, int WK>
 __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const TrackParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Tables tb = stage_tables(smem, p.hx_terms, p.hx_off, p.ht_terms, p.ht_off, N, p.n_hx_terms, p.n_ht_terms);
@@ -800,7 +818,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
   const int l = lane % W;
   const int g = threadIdx.x / W;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
-  const int walk = (kFlatAlways<N> && p.flat_eval == 0) ? 1 : p.flat_eval;
+  const int walk = WK >= 0 ? WK : ((kFlatAlways<N> && p.flat_eval == 0) ? 1 : p.flat_eval);
   const bool flat = walk != 0;
   SubMem sm = sub_layout<R, RL>(smem + tables_bytes(N, p.n_hx_terms, p.n_ht_terms) +
                                     (size_t)g * sub_bytes(N, Mc, W, flat ? p.scr_slots : 0, (int)sizeof(cx<RL>),

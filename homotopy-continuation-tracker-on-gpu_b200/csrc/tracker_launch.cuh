@@ -28,10 +28,10 @@ inline int block_threads(size_t tables, size_t per_sub, int W) {
   return 0;
 }
 
-template <typename R, typename RL, int N, int KIND, int V, int S>
-int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
+template <typename R, typename RL, int N, int KIND, int V, int S, int WK>
+int launch_track_w(const TrackParams& p, cudaStream_t s, int n_sm) {
   constexpr int W = (N <= 4) ? 4 : (N <= 8) ? 8 : (N <= 16) ? 16 : 32;
-  auto kern = dev::track_kernel<R, RL, N, W, KIND, V, S>;
+  auto kern = dev::track_kernel<R, RL, N, W, KIND, V, S, WK>;
   const int Mc = (KIND == KIND_P2C) ? p.M + 1 : p.P + 1;
   const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
   const size_t tables = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms);
@@ -83,6 +83,17 @@ int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
   kern<<<(unsigned)grid, block, smem, s>>>(q);
   e = cudaGetLastError();
   return e == cudaSuccess ? 0 : -23;
+}
+
+// above 16 unknowns one kernel per H_x walk (row-wise, balanced), else the walk is chosen at run time
+template <typename R, typename RL, int N, int KIND, int V, int S>
+int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
+  if constexpr (N > 16) {
+    if (p.flat_eval == 2 && balanced_walk_built(N)) return launch_track_w<R, RL, N, KIND, V, S, 2>(p, s, n_sm);
+    return launch_track_w<R, RL, N, KIND, V, S, 1>(p, s, n_sm);
+  } else {
+    return launch_track_w<R, RL, N, KIND, V, S, -1>(p, s, n_sm);
+  }
 }
 
 template <typename R, typename RL, int N, int KIND, int V>

@@ -426,7 +426,7 @@ def test_single_instance_spread_equals_batch(name, precision):
         oargs = {k: (v.astype(np.complex64) if isinstance(v, np.ndarray) else v) for k, v in oargs.items()}
         r = O.track(ob, ob.start_sols.astype(np.complex64), precision="f", nthreads=NCPU, **oargs)
     elif precision == ghc.PREC_MIXED:
-        r = O.track(ob, ob.start_sols, precision="mixed", t_switch=0.9, nthreads=NCPU, **oargs)
+        r = O.track(ob, ob.start_sols, precision="mixed", nthreads=NCPU, **oargs)
     else:
         r = O.track(ob, ob.start_sols, nthreads=NCPU, **oargs)
     compare(one, r)

@@ -162,6 +162,7 @@ int track_params(const Problem& pb, const ghc_track_args* a, TrackParams& p) {
   if (a->first_tol2 > 0) p.first_tol2 = a->first_tol2;
   if (a->dt_max > 0) p.dt_max = a->dt_max;
   if (a->cond_limit > 0) p.cond_limit = a->cond_limit;
+  if (a->dt_floor > 0) p.dt_floor = a->dt_floor;
   return GHC_OK;
 }
 

@@ -184,8 +184,9 @@ struct TrackParams {
   double first_tol2;  // reject when the first Newton update has |dx|^2 > first_tol2 |x|^2
   double dt_max;      // step-size cap
   // mixed tracker: stop a path (handover) after a step in which a solve's pivot magnitudes spanned
-  // more than cond_limit, or one was NaN (0: never)
+  // more than cond_limit, or one was NaN (0: never), or once its step falls below dt_floor (0: never)
   double cond_limit;
+  double dt_floor;
 };
 
 struct PolishParams {

@@ -12,9 +12,11 @@
 // set by the FP32 solve, about cond(H_x) times FP32's rounding).  It takes every
 // path to t = 1 (or to t_switch, when t_switch < 1); a path stops early after a
 // step in which an FP32 solve's pivot magnitudes spanned more than cond_limit
-// (the Jacobian is too ill-conditioned for FP32: Newton would stall), after
-// kMixedFailLimit failed steps in a row, or on divergence (then at its last
-// accepted point), with t, dt and its step and corrector counts in t_end,
+// (the Jacobian is too ill-conditioned for FP32: Newton would stall), once its
+// step falls below dt_floor (FP32 keeps failing the corrector where FP64 would
+// not: a few per cent of paths near t = 1 otherwise crawl to the step cap),
+// after kMixedFailLimit failed steps in a row, or on divergence (then at its
+// last accepted point), with t, dt and its step and corrector counts in t_end,
 // dt_end, steps and corr.  The FP64 tracker then resumes every
 // path from there: a path the mixed tracker finished stops at once, a handed-over
 // one continues with FP64 linear algebra (ill-conditioned Jacobians near a
@@ -36,13 +38,15 @@ int track_subwarp_width(int N) {
 }
 
 constexpr int kMixedFailLimit = 4;
-constexpr double kMixedCondLimit = 1e4;
+constexpr double kMixedCondLimit = 1e5;
+constexpr double kMixedDtFloor = 1e-4;
 
 int launch_track(const TrackParams& p, int precision, double t_switch, void* stream, int n_sm) {
   cudaStream_t s = (cudaStream_t)stream;
   if (p.n_items <= 0) return 0;
   TrackParams q = p;
-  q.cond_limit = 0.0;  // the plain trackers never stop on conditioning
+  q.cond_limit = 0.0;  // the plain trackers never stop on conditioning or step size
+  q.dt_floor = 0.0;
   switch (precision) {
     case PREC_FP64:
       return launch_track_fp64(q, s, n_sm);
@@ -55,6 +59,7 @@ int launch_track(const TrackParams& p, int precision, double t_switch, void* str
       a.t_handover = t_switch < 1.0 ? t_switch : 0.0;  // 0: no time boundary, the whole path
       a.fail_limit = kMixedFailLimit;
       a.cond_limit = p.cond_limit > 0.0 ? p.cond_limit : kMixedCondLimit;
+      a.dt_floor = p.dt_floor > 0.0 ? p.dt_floor : kMixedDtFloor;
       a.variant = p.variant_f32;
       a.flat_eval = p.flat_eval_f32;
       int rc = launch_track_mixed(a, s, n_sm);

@@ -756,7 +756,7 @@ __device__ __forceinline__ cx<R> load_cx(const void* base, bool f64, long long i
 template <int N, typename R, typename RL, int V>
 constexpr int track_min_blocks() {
   return !std::is_same<R, RL>::value
-             ? (V == 0 ? (N <= 8 ? 6 : N <= 12 ? 6 : N <= 18 ? 4 : 4) : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 5 : 3))
+             ? (V == 0 ? (N <= 8 ? 6 : N <= 12 ? 6 : N <= 18 ? 4 : 4) : (N <= 8 ? 8 : N <= 12 ? 5 : N <= 18 ? 5 : 3))
          : V == 0 ? (sizeof(R) == 8 ? (N <= 4 ? 6 : N <= 8 ? 4 : N <= 12 ? 5 : 3)
                                     : (N <= 8 ? 8 : N <= 12 ? 7 : N <= 18 ? 4 : 5))
                   : (sizeof(R) == 8 ? (N <= 4 ? 8 : N <= 8 ? 6 : N <= 12 ? 4 : N <= 18 ? 4 : 2)
@@ -1052,7 +1052,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
         }
       }
       ++step;
-      if (step_ill) ill_stop = true;
+      if (step_ill || (p.dt_floor > 0.0 && (double)dt < p.dt_floor)) ill_stop = true;
       last_sing = step_sing;
       if (!done) done = at_end();
       if (done && !inf && p.t_handover > 0.0 && f_sub(t_hand, t0) <= R(1e-6) && step <= p.max_steps &&

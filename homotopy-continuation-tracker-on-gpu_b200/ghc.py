@@ -55,7 +55,8 @@ class TrackArgs(ctypes.Structure):
                 ("d_start_sols", _P), ("d_coef_hx", _P), ("d_coef_ht", _P), ("d_p_start", _P),
                 ("d_p_target", _P), ("d_p_diff", _P), ("d_endpoints", _P), ("d_status", _P), ("d_conv", _P),
                 ("d_inf", _P), ("d_steps", _P), ("d_corr", _P), ("d_t_end", _P), ("d_dt_end", _P),
-                ("d_resid", _P), ("d_counter", _P), ("paths", _I32), ("cond_limit", ctypes.c_double)]
+                ("d_resid", _P), ("d_counter", _P), ("paths", _I32), ("cond_limit", ctypes.c_double),
+                ("dt_floor", ctypes.c_double)]
 
 
 def _sig(name, res, args):
@@ -227,17 +228,18 @@ class Workspace:
 
 def track(pb, ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, d_p_target=None, d_p_diff=None,
           t_switch=1.0, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False, step=None,
-          no_alloc=False, cond_limit=0.0):
+          no_alloc=False, cond_limit=0.0, dt_floor=0.0):
     """Launch the batched tracker (asynchronous on torch's current stream).
 
     step: optional dict(corr_tol2=, first_tol2=, dt_max=) step control; the
     default is the reference's (see ROBUST_STEP for the path-jump-free one).
     PREC_MIXED: the mixed tracker (FP64 state and residual, FP32 H_x, H_t and LU) for
     t < t_switch (>= 1: the whole path), then FP64 for the paths it hands over
-    (cond_limit: pivot-magnitude span of an FP32 solve that hands a path over, 0: 1e4).
+    (cond_limit: pivot-magnitude span of an FP32 solve that hands a path over, 0: 1e5;
+    dt_floor: step size below which a path is handed over, 0: 1e-4).
     """
     a = _track_args(ws, d_start_sols, d_coef_hx, d_coef_ht, d_p_start, d_p_target, d_p_diff, t_switch,
-                    polish_iters, max_steps, max_corr, incr_steps, want_resid, step, cond_limit)
+                    polish_iters, max_steps, max_corr, incr_steps, want_resid, step, cond_limit, dt_floor)
     if no_alloc:
         # ghc_track_noalloc: counter and tables in the library's fixed device array
         a.d_counter = None
@@ -271,7 +273,7 @@ def get_tuning(pb, precision):
 
 def _track_args(ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, d_p_target=None, d_p_diff=None,
                 t_switch=1.0, polish_iters=0, max_steps=0, max_corr=0, incr_steps=0, want_resid=False, step=None,
-                cond_limit=0.0):
+                cond_limit=0.0, dt_floor=0.0):
     a = TrackArgs()
     a.n_hyp = ws.n_hyp
     a.precision = ws.precision
@@ -293,6 +295,7 @@ def _track_args(ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None
     a.d_counter = ws.counter.data_ptr()
     a.paths = ws.paths
     a.cond_limit = cond_limit
+    a.dt_floor = dt_floor
     return a
 
 

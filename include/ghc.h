@@ -125,9 +125,9 @@ typedef struct {
   double t_switch;            /* GHC_PREC_MIXED: the mixed tracker (FP64 track, t, step control and corrector
                                  residual H; FP32 H_x, H_t and LU) for t < t_switch (>= 1: to t = 1;
                                  <= 0: all FP64); a path goes on in FP64 after a step whose FP32 solve had
-                                 pivot magnitudes spanning more than cond_limit, after 4 failed steps in a
-                                 row, or on divergence (at its last accepted point); needs d_steps, d_corr,
-                                 d_t_end, d_dt_end */
+                                 pivot magnitudes spanning more than cond_limit, once its step falls below
+                                 dt_floor, after 4 failed steps in a row, or on divergence (at its last
+                                 accepted point); needs d_steps, d_corr, d_t_end, d_dt_end */
   int32_t polish_iters;       /* Newton iterations at t = 1 after tracking (FP64 state only) */
   /* step control; <= 0 selects the reference's value (kernel_HC_Solver_P3P.cu:214) */
   double corr_tol2;           /* corrector success |dx|^2 < corr_tol2 |x|^2 (reference 1e-6) */
@@ -155,8 +155,9 @@ typedef struct {
   /* start solutions per hypothesis in d_start_sols; <= 0: the problem's Num_Of_Tracks */
   int32_t paths;
   /* GHC_PREC_MIXED: the pivot-magnitude span max|U_ii| / min|U_ii| of an FP32 solve above which the
-     path goes on in FP64 (<= 0: 1e4) */
+     path goes on in FP64 (<= 0: 1e5), and the step size below which it does (<= 0: 1e-4) */
   double cond_limit;
+  double dt_floor;
 } ghc_track_args;
 
 int ghc_track(const ghc_problem* pb, const ghc_track_args* args, void* stream);

@@ -49,6 +49,8 @@ typedef struct {
   /* mixed tracker: hand a path over after a step in which a float solve's pivot magnitudes spanned
    * more than cond_limit (0: never) */
   double cond_limit;
+  /* mixed tracker: hand a path over once its step falls below dt_floor (0: never) */
+  double dt_floor;
 } orc_problem;
 
 typedef struct {

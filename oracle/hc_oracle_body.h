@@ -447,6 +447,7 @@ static void SFX(track_path)(const HYP* h, CX* x_io, orc_path_out* out) {
       }
     }
     if (ill) ill_stop = 1;
+    if (pb->dt_floor > 0 && (double)dt < pb->dt_floor) ill_stop = 1; /* mixed: steps this small mean float is stuck */
     last_sing = step_sing;
   }
 

@@ -213,7 +213,7 @@ class _Prob(ctypes.Structure):
                 ("hx_idx", ctypes.c_void_p), ("ht_idx", ctypes.c_void_p), ("corr_tol2", ctypes.c_double),
                 ("first_tol2", ctypes.c_double), ("dt_max", ctypes.c_double),
                 ("t_handover", ctypes.c_double), ("fail_limit", ctypes.c_int32), ("resume", ctypes.c_int32),
-                ("cond_limit", ctypes.c_double)]
+                ("cond_limit", ctypes.c_double), ("dt_floor", ctypes.c_double)]
 
 # step control of the reference (kernel_HC_Solver_P3P.cu:214, no contraction test, no dt cap)
 REFERENCE_STEP = dict(corr_tol2=1e-6, first_tol2=float("inf"), dt_max=float("inf"))
@@ -260,15 +260,16 @@ def _prob_struct(pb, polish_iters, max_steps=None, max_corr=None, incr=None, ste
 
 # the tracker library's two-phase mixed precision (csrc/tracker.cu): the mixed tracker (double state,
 # residual and step control, float H_x, H_t and LU) to t = 1 or t_switch < 1, a path handed over after
-# a step whose float solve had pivot magnitudes spanning more than cond_limit, after 4 failed steps in
-# a row, or on divergence; then the double tracker resumes every path
+# a step whose float solve had pivot magnitudes spanning more than cond_limit, once its step falls below
+# dt_floor, after 4 failed steps in a row, or on divergence; then the double tracker resumes every path
 MIXED_FAIL_LIMIT = 4
-MIXED_COND_LIMIT = 1e4
+MIXED_COND_LIMIT = 1e5
+MIXED_DT_FLOOR = 1e-4
 
 
 def track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precision="d",
           polish_iters=0, nthreads=0, max_steps=None, max_corr=None, incr=None, step=None, t_switch=1.0,
-          cond_limit=MIXED_COND_LIMIT):
+          cond_limit=MIXED_COND_LIMIT, dt_floor=MIXED_DT_FLOOR):
     """Track all start paths for H hypotheses.
 
     P2C: hx [H, (M+1)(K+1)], ht [H, (M+1)K] complex.
@@ -285,7 +286,7 @@ def track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precisi
     if not t_switch > 0:
         return _track(pb, start_sols, precision="d", polish_iters=polish_iters, **kw)
     first = _track(pb, start_sols, precision="m", polish_iters=0,
-                   handover=(t_switch if t_switch < 1 else 0.0, MIXED_FAIL_LIMIT, cond_limit), **kw)
+                   handover=(t_switch if t_switch < 1 else 0.0, MIXED_FAIL_LIMIT, cond_limit, dt_floor), **kw)
     return _track(pb, start_sols, precision="d", polish_iters=polish_iters, resume=first, **kw)
 
 
@@ -324,6 +325,8 @@ def _track(pb, start_sols, hx=None, ht=None, p_start=None, p_target=None, precis
         s.t_handover, s.fail_limit = handover[:2]
         if len(handover) > 2:
             s.cond_limit = handover[2]
+        if len(handover) > 3:
+            s.dt_floor = handover[3]
     if resume is not None:
         s.resume = 1
         ep[...] = resume["endpoints_raw"].astype(rt)

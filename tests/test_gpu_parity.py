@@ -169,25 +169,27 @@ def test_mixed_handover_happens():
     ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_MIXED, t_switch=0.5, max_steps=6)
     r_mixed = O.track(ob, ob.start_sols, precision="mixed", t_switch=0.5, max_steps=6, nthreads=NCPU, **oargs)
     compare(ws, r_mixed)
-    first = O._track(ob, ob.start_sols, precision="m", max_steps=6, handover=(0.5, O.MIXED_FAIL_LIMIT,
-                                                                               O.MIXED_COND_LIMIT), **oargs)
+    first = O._track(ob, ob.start_sols, precision="m", max_steps=6,
+                     handover=(0.5, O.MIXED_FAIL_LIMIT, O.MIXED_COND_LIMIT, O.MIXED_DT_FLOOR), **oargs)
     assert (first["t_end"] <= 0.5 + 1e-6).all()
     assert (ws.steps.cpu().numpy() >= first["steps"]).all()
 
 
-@pytest.mark.parametrize("name,cond_limit", [("generalized_3views_4pts", 1e3), ("generalized_3views_4pts", 1e5),
-                                             ("uncalibrated_trifocal_rel_pos_CY", 1e4),
-                                             ("trifocal_2op1p_30x30", 1e4)])
-def test_mixed_conditioning_handover_bit_exact(name, cond_limit):
+@pytest.mark.parametrize("name,cond_limit,dt_floor", [("generalized_3views_4pts", 1e3, 1e-4),
+                                                      ("generalized_3views_4pts", 1e5, 1e-4),
+                                                      ("generalized_3views_4pts", 1e7, 1e-3),
+                                                      ("uncalibrated_trifocal_rel_pos_CY", 1e5, 1e-4),
+                                                      ("trifocal_2op1p_30x30", 1e5, 1e-4)])
+def test_mixed_conditioning_handover_bit_exact(name, cond_limit, dt_floor):
     """The mixed tracker to t = 1 under the path-jump-free control, handing a path to FP64 after a
-    step whose FP32 solve had a pivot-magnitude span above cond_limit: both phases equal the
-    oracle's bit for bit, and some paths do take the FP64 phase."""
+    step whose FP32 solve had a pivot-magnitude span above cond_limit or once its step falls below
+    dt_floor: both phases equal the oracle's bit for bit, and some paths do take the FP64 phase."""
     pb, ob, tg = inputs(name, n_hyp=2, seed=7)
-    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=2, cond_limit=cond_limit, **ROBUST)
+    ws, oargs = run_gpu(pb, ob, tg, ghc.PREC_MIXED, polish=2, cond_limit=cond_limit, dt_floor=dt_floor, **ROBUST)
     r = O.track(ob, ob.start_sols, precision="mixed", polish_iters=2, nthreads=NCPU, cond_limit=cond_limit,
-                step=O.ROBUST_STEP, max_corr=3, max_steps=2000, **oargs)
+                dt_floor=dt_floor, step=O.ROBUST_STEP, max_corr=3, max_steps=2000, **oargs)
     compare(ws, r)
-    first = O._track(ob, ob.start_sols, precision="m", handover=(0.0, O.MIXED_FAIL_LIMIT, cond_limit),
+    first = O._track(ob, ob.start_sols, precision="m", handover=(0.0, O.MIXED_FAIL_LIMIT, cond_limit, dt_floor),
                      step=O.ROBUST_STEP, max_corr=3, max_steps=2000, nthreads=NCPU, **oargs)
     assert 0 < (first["conv"] == 0).sum() < first["conv"].size
 

@@ -53,7 +53,7 @@ def test_no_alloc_matches_track_on_two_calls(name, n_hyp, prec):
     """The first call comes on a fresh problem handle, which must stay unbound to any device
     afterwards (nothing was uploaded into it); both calls must equal ghc_track's results,
     computed afterwards on a second handle of the same problem."""
-    fresh = ghc.Problem(name)
+    fresh, other = ghc.Problem(name), ghc.Problem(name)
     s, t = fresh.params()
     rng = np.random.default_rng(17)
     tg = np.array([np.append(t[:-1] + 0.05 * (rng.normal(size=fresh.P) + 1j * rng.normal(size=fresh.P)), 1.0)
@@ -61,7 +61,8 @@ def test_no_alloc_matches_track_on_two_calls(name, n_hyp, prec):
     rt = torch.float32 if prec == ghc.PREC_FP32 else torch.float64
     sols = cx_t(fresh.start_sols()).to(rt)
     if fresh.kind == ghc.KIND_P2C:
-        hx, ht = fresh.p2c_device(cx_t(s), cx_t(tg))
+        # the coefficient tables come from the other handle (device P2C uploads into its handle)
+        hx, ht = other.p2c_device(cx_t(s), cx_t(tg))
         kw = dict(d_coef_hx=hx, d_coef_ht=ht)
     else:
         kw = dict(d_p_start=cx_t(s), d_p_target=cx_t(tg), d_p_diff=cx_t(tg - s[None, :]))
@@ -73,7 +74,6 @@ def test_no_alloc_matches_track_on_two_calls(name, n_hyp, prec):
         torch.cuda.synchronize()
         got.append(outputs(ws))
     assert fresh.bound_device() == -1
-    other = ghc.Problem(name)
     ref_ws = ghc.Workspace(other, n_hyp, prec)
     ghc.track(other, ref_ws, sols, polish_iters=polish, **kw)
     torch.cuda.synchronize()

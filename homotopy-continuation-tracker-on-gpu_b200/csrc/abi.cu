@@ -188,11 +188,13 @@ using namespace ghc;
 
 namespace {
 
-// Pointer array of the reference layout: entry p == base + p * (N+1) complex.
+// Pointer array of the reference layout: entry p == base + p * (N+1) complex.  Read on the
+// caller's stream (after the work the caller queued there), then checked on the host.
 template <typename T>
-int regular_base(T* const* d_ptrs, long long n, int N, T** base) {
+int regular_base(T* const* d_ptrs, long long n, int N, T** base, cudaStream_t st) {
   std::vector<T*> h((size_t)n);
-  if (cudaMemcpy(h.data(), d_ptrs, n * sizeof(T*), cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (cudaMemcpyAsync(h.data(), d_ptrs, n * sizeof(T*), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
     return cuda_fail("copy of pointer array");
   for (long long i = 0; i < n; ++i) {
     if (h[i] != h[0] + 2 * i * (N + 1)) {
@@ -204,44 +206,50 @@ int regular_base(T* const* d_ptrs, long long n, int N, T** base) {
   return GHC_OK;
 }
 
-// Tables passed to a drop-in wrapper: the handle's compiled copy when they are
-// identical to the files it loaded, else compiled now into `tmp` device memory.
-int dropin_tables(Problem& pb, const int* d_hx, const int* d_ht, TrackParams& p, std::vector<void*>& tmp) {
+// Tables passed to a drop-in wrapper, read on the caller's stream: the handle's compiled copy when
+// they are identical to the files it loaded; else their compiled copy kept in the handle, compiled
+// and uploaded (on the caller's stream) only when they differ from the last such tables.
+int dropin_tables(Problem& pb, const int* d_hx, const int* d_ht, TrackParams& p, cudaStream_t st) {
   std::vector<int32_t> hx(pb.hx_raw.size()), ht(pb.ht_raw.size());
-  if (cudaMemcpy(hx.data(), d_hx, hx.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(ht.data(), d_ht, ht.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (cudaMemcpyAsync(hx.data(), d_hx, hx.size() * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(ht.data(), d_ht, ht.size() * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
     return cuda_fail("copy of index tables");
   if (hx == pb.hx_raw && ht == pb.ht_raw) return GHC_OK;
-  std::vector<uint64_t> hxt, htt;
-  std::vector<uint16_t> hxo, hto;
-  int rc = compile_tables(hx, ht, pb, hxt, hxo, htt, hto);
-  if (rc) return rc;
-  void *a, *b, *c, *d;
-  if (cudaMalloc(&a, std::max<size_t>(1, hxt.size()) * 8) || cudaMalloc(&b, hxo.size() * 2) ||
-      cudaMalloc(&c, std::max<size_t>(1, htt.size()) * 8) || cudaMalloc(&d, hto.size() * 2))
-    return cuda_fail("table upload");
-  tmp.insert(tmp.end(), {a, b, c, d});
-  cudaMemcpy(a, hxt.data(), hxt.size() * 8, cudaMemcpyHostToDevice);
-  cudaMemcpy(b, hxo.data(), hxo.size() * 2, cudaMemcpyHostToDevice);
-  cudaMemcpy(c, htt.data(), htt.size() * 8, cudaMemcpyHostToDevice);
-  cudaMemcpy(d, hto.data(), hto.size() * 2, cudaMemcpyHostToDevice);
-  p.hx_terms = (const uint64_t*)a;
-  p.hx_off = (const uint16_t*)b;
-  p.ht_terms = (const uint64_t*)c;
-  p.ht_off = (const uint16_t*)d;
-  p.n_hx_terms = (int)hxt.size();
-  p.n_ht_terms = (int)htt.size();
-  p.flat_eval = flat_eval_pays(hxo.data(), pb.N);  // the caller's own tables: their own walk
-  p.scr_slots = row_nonzeros_max(hxo.data(), pb.N);
+  CallerTables& c = pb.dev.caller;
+  if (!(c.dev[0] && hx == c.hx_raw && ht == c.ht_raw)) {
+    CallerTables fresh;
+    int rc = compile_tables(hx, ht, pb, fresh.hx_terms, fresh.hx_off, fresh.ht_terms, fresh.ht_off);
+    if (rc) return rc;
+    c.release();
+    c = std::move(fresh);
+    c.hx_raw = hx;
+    c.ht_raw = ht;
+    const size_t bytes[4] = {std::max<size_t>(1, c.hx_terms.size()) * 8, c.hx_off.size() * 2,
+                             std::max<size_t>(1, c.ht_terms.size()) * 8, c.ht_off.size() * 2};
+    const void* src[4] = {c.hx_terms.data(), c.hx_off.data(), c.ht_terms.data(), c.ht_off.data()};
+    const size_t used[4] = {c.hx_terms.size() * 8, c.hx_off.size() * 2, c.ht_terms.size() * 8, c.ht_off.size() * 2};
+    for (int k = 0; k < 4; ++k) {
+      if (cudaMalloc(&c.dev[k], bytes[k]) != cudaSuccess) {
+        c.release();
+        return cuda_fail("table upload");
+      }
+      if (used[k] && cudaMemcpyAsync(c.dev[k], src[k], used[k], cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        c.release();
+        return cuda_fail("table upload");
+      }
+    }
+  }
+  p.hx_terms = (const uint64_t*)c.dev[0];
+  p.hx_off = (const uint16_t*)c.dev[1];
+  p.ht_terms = (const uint64_t*)c.dev[2];
+  p.ht_off = (const uint16_t*)c.dev[3];
+  p.n_hx_terms = (int)c.hx_terms.size();
+  p.n_ht_terms = (int)c.ht_terms.size();
+  p.flat_eval = flat_eval_pays(c.hx_off.data(), pb.N);  // the caller's own tables: their own walk
+  p.scr_slots = row_nonzeros_max(c.hx_off.data(), pb.N);
   return GHC_OK;
 }
-
-struct TmpFree {
-  std::vector<void*> v;
-  ~TmpFree() {
-    for (void* p : v) cudaFree(p);
-  }
-};
 
 // Shared body of the four drop-in wrappers.  Real = float or double.
 template <typename Real>
@@ -258,13 +266,14 @@ double dropin(const ghc_problem* h, void* stream, int max_steps, int max_corr, i
   if (rc) return rc;
   const bool fp32 = std::is_same<Real, float>::value;
   const long long n = pb.paths;
+  cudaStream_t st = (cudaStream_t)stream;
   Real *start_base, *track_base;
-  if ((rc = regular_base(d_start_arr, n, pb.N, &start_base)) || (rc = regular_base(d_track_arr, n, pb.N, &track_base)))
+  if ((rc = regular_base(d_start_arr, n, pb.N, &start_base, st)) ||
+      (rc = regular_base(d_track_arr, n, pb.N, &track_base, st)))
     return rc;
   TrackParams p = base_params(pb);
   apply_tuning(pb, fp32 ? PREC_FP32 : PREC_FP64, p);
-  TmpFree tmp;
-  if ((rc = dropin_tables(pb, d_hx, d_ht, p, tmp.v))) return rc;
+  if ((rc = dropin_tables(pb, d_hx, d_ht, p, st))) return rc;
   p.max_steps = max_steps;
   p.max_corr = max_corr;
   p.incr = incr;
@@ -290,7 +299,6 @@ double dropin(const ghc_problem* h, void* stream, int max_steps, int max_corr, i
   double* d_pd = d_pt + npar;
   double* d_t = d_pd + npar;
   double* d_dt = d_t + n;
-  cudaStream_t st = (cudaStream_t)stream;
   auto to_double = [&](const Real* src, double* dst, long long cnt) -> int {
     if (cnt <= 0) return 0;
     if (fp32) return launch_f2d((const float*)src, dst, cnt, stream);

@@ -86,6 +86,13 @@ bool read_ints(const std::string& path, std::vector<int32_t>& out) {
 void set_error(const std::string& msg) { g_err = msg; }
 const char* last_error() { return g_err.c_str(); }
 
+void CallerTables::release() {
+  for (void*& d : dev) {
+    if (d) cudaFree(d);
+    d = nullptr;
+  }
+}
+
 Problem::~Problem() {
   if (dev.device >= 0) {
     int cur = 0;
@@ -105,6 +112,7 @@ Problem::~Problem() {
     cudaFree(dev.solve_arena);
     if (dev.solve_stream) cudaStreamDestroy((cudaStream_t)dev.solve_stream);
     cudaFree(dev.counter);
+    dev.caller.release();
     cudaSetDevice(cur);
   }
 }

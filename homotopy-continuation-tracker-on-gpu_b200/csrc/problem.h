@@ -15,6 +15,17 @@ struct P2CTerm {
   std::vector<int> fac;  // parameter indices (0-based), with repetition
 };
 
+// Index tables a drop-in wrapper was handed that differ from the loaded ones: the caller's raw
+// tables, their compiled form (host copies, which stay alive while their upload is queued) and the
+// device copies (hx terms, hx offsets, ht terms, ht offsets).
+struct CallerTables {
+  std::vector<int32_t> hx_raw, ht_raw;
+  std::vector<uint64_t> hx_terms, ht_terms;
+  std::vector<uint16_t> hx_off, ht_off;
+  void* dev[4] = {nullptr, nullptr, nullptr, nullptr};
+  void release();
+};
+
 struct DeviceTables {
   int device = -1;
   uint64_t* hx_terms = nullptr;
@@ -36,6 +47,7 @@ struct DeviceTables {
   size_t solve_bytes = 0;
   void* solve_stream = nullptr;
   int* counter = nullptr;
+  CallerTables caller;
 };
 
 struct Problem {

@@ -852,7 +852,9 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
   R t0 = 0, dt = 0, t_step = 0, half = 0, dt_pre = 0;
   R coef_t = R(-1);  // the t at which this sub-warp's coefficient buffers hold c_k(t) (-1: none)
   bool end_zone = false, success = false, inf = false, finished = false;
-  bool step_ill = false, ill_stop = false;  // mixed: a solve of this step was ill-conditioned; stop after it
+  // mixed tracker only: a solve of this step was ill-conditioned, or the step fell below the floor: stop
+  constexpr bool kMixed = !std::is_same<R, RL>::value;
+  bool step_ill = false, ill_stop = false;
   bool step_sing = false, last_sing = false;  // a solve of this step / the last completed step had a zero pivot
   int nsucc = 0, step = 0, ncorr = 0, phase = 0, cit = 0, nfail = 0;
   const R dt_init = (KIND == KIND_PH) ? R(0.01) : R(0.05);
@@ -880,7 +882,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
   auto at_end = [&]() -> bool {
     return !(t0 < R(1) && f_sub(R(1), t0) > R(1e-7)) || step > p.max_steps ||
            (p.t_handover > 0.0 && f_sub(t_hand, t0) <= R(1e-6)) || (p.fail_limit > 0 && nfail >= p.fail_limit) ||
-           ill_stop;
+           (kMixed && ill_stop);
   };
   auto init_path = [&](long long it) {
     hyp = it / p.paths_per_hyp;
@@ -985,7 +987,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
     bool ill = false, sing = false;
     const cx<R> v = eval_solve<R, RL, N, W, KIND, S>(tb, sm, l, rk ? 1 : 0, p.cond_limit, ill, sing);
     unstash();
-    if (served && ill) step_ill = true;
+    if (kMixed && served && ill) step_ill = true;
     if (served && sing) step_sing = true;
     // ---------------- corrector norms (kernel_HC_Solver_P3P.cu:204-219), all lanes take part
     R ns0 = 0, nc0 = 0;
@@ -1052,7 +1054,7 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
         }
       }
       ++step;
-      if (step_ill || (p.dt_floor > 0.0 && (double)dt < p.dt_floor)) ill_stop = true;
+      if (kMixed && (step_ill || (p.dt_floor > 0.0 && (double)dt < p.dt_floor))) ill_stop = true;
       last_sing = step_sing;
       if (!done) done = at_end();
       if (done && !inf && p.t_handover > 0.0 && f_sub(t_hand, t0) <= R(1e-6) && step <= p.max_steps &&

@@ -432,3 +432,41 @@ def test_single_instance_spread_equals_batch(name, precision):
     else:
         r = O.track(ob, ob.start_sols, nthreads=NCPU, **oargs)
     compare(one, r)
+
+
+def test_dropin_caller_tables_differ_from_loaded():
+    """A drop-in call handed index tables that differ from the problem folder's (here the terms of
+    every H_x entry in reverse order: the same system, another summation order) tracks with those
+    tables -- compiled once and kept in the handle, so a second call reuses them -- and equals the
+    oracle reading the same tables; the handle's own tables serve a later call with the loaded ones."""
+    pb, ob, tg = inputs("P3P")
+    N, n = pb.N, pb.paths
+    rev = np.ascontiguousarray(ob.hx_idx.reshape(N, N, ob.Tx, ob.Px)[:, :, ::-1, :].reshape(-1))
+    hx, ht = O.p2c_tables(ob.terms, ob.start_params, ob.target_params)
+    keep = [cx_t(hx), cx_t(ht)]
+    st = torch.cuda.current_stream().cuda_stream
+    sols = np.concatenate([ob.start_sols, np.ones((n, 1))], axis=1)
+
+    def call(hx_idx):
+        d_start, d_track = cx_t(sols), cx_t(sols)
+        ps = torch.tensor([d_start.data_ptr() + i * (N + 1) * 16 for i in range(n)], dtype=torch.int64).cuda()
+        pt = torch.tensor([d_track.data_ptr() + i * (N + 1) * 16 for i in range(n)], dtype=torch.int64).cuda()
+        d_hxi, d_hti = torch.from_numpy(hx_idx).cuda(), torch.from_numpy(ob.ht_idx).cuda()
+        conv = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        inf = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        sec = ghc.ghc_kernel_HC_Solver_P2C_z(pb.h, st, pb.max_steps, pb.max_corr, pb.incr_steps, ps.data_ptr(),
+                                             pt.data_ptr(), d_hxi.data_ptr(), d_hti.data_ptr(), keep[0].data_ptr(),
+                                             keep[1].data_ptr(), conv.data_ptr(), inf.data_ptr(), None)
+        assert sec >= 0, ghc.ghc_last_error()
+        return to_cx(d_track)[:, :N], conv.cpu().numpy()
+
+    loaded = ob.hx_idx
+    ob.hx_idx = rev
+    r = O.track(ob, ob.start_sols, hx=hx, ht=ht, nthreads=NCPU)
+    ob.hx_idx = loaded
+    r0 = O.track(ob, ob.start_sols, hx=hx, ht=ht, nthreads=NCPU)
+    for _ in range(2):
+        ep, conv = call(rev)
+        assert np.array_equal(conv, r["conv"]) and np.array_equal(ep, r["endpoints"])
+    ep, conv = call(np.ascontiguousarray(loaded))
+    assert np.array_equal(conv, r0["conv"]) and np.array_equal(ep, r0["endpoints"])

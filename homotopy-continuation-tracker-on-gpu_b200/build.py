@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "-I", os.path.join(REPO, "include")]
 LIB_SOURCES = ["tracker.cu", "tracker_fp64.cu", "tracker_fp64_v1.cu", "tracker_fp32.cu", "tracker_fp32_v1.cu", "tracker_mixed.cu", "tracker_mixed_v1.cu", "p2c.cu", "results.cu", "abi.cu",
-               "peak.cu", "no_alloc.cu", "linsolve.cu", "problem.cpp"]
+               "peak.cu", "no_alloc.cu", "linsolve.cu", "mix.cu", "problem.cpp"]
 HEADERS = ["ghc_internal.h", "tracker.cuh", "tracker_launch.cuh", "problem.h", "abi_internal.h"]
 
 

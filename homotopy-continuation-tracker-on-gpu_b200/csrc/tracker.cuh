@@ -809,9 +809,14 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 // WK >= 0: the H_x walk is fixed at compile time (only that walk's code is in the kernel, which
 // spares the register allocator the other walk's read-back: above 16 unknowns, where the row fills
 // most of the registers); WK < 0: chosen at run time from p.flat_eval.
-template <typename R, typename RL, int N, int W, int KIND, int V, int S, int WK>
-__global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const TrackParams p) {
-  extern __shared__ __align__(16) unsigned char smem[];
+//
+// track_body is the work of one CTA on the items of p: CTA number `cta` of the `n_cta` CTAs that
+// serve p (first items static: one per sub-warp slot of the CTA; then the shared counter), or,
+// as a `visitor` (a CTA of another bucket of a mixed launch whose own items are done), items
+// from p's counter only.  smem: the CTA's dynamic shared memory.
+template <typename R, typename RL, int N, int W, int KIND, int S, int WK>
+__device__ __forceinline__ void track_body(const TrackParams& p, unsigned char* smem, long long cta, long long n_cta,
+                                           bool visitor) {
   const Tables tb = stage_tables(smem, p.hx_terms, p.hx_off, p.ht_terms, p.ht_off, N, p.n_hx_terms, p.n_ht_terms);
 
   const int lane = threadIdx.x & 31;
@@ -837,15 +842,19 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
   // shared memory); only the first one (primary) writes results and takes the next path.
   const int subs_per_cta = blockDim.x / W;
   const int slots_per_cta = p.spread ? (int)(blockDim.x / 32) : subs_per_cta;
-  const long long n_sw = (long long)gridDim.x * slots_per_cta;
+  const long long n_sw = n_cta * slots_per_cta;
   const bool primary = !p.spread || lane < W;
   const int leader = lane - l;
   const bool handover = p.t_handover > 0.0 || p.fail_limit > 0;
   const R t_hand = (R)p.t_handover;
 
   // per-path state (replicated across the sub-warp's lanes)
-  long long item = p.spread ? (long long)blockIdx.x * slots_per_cta + (threadIdx.x >> 5)
-                            : (long long)blockIdx.x * subs_per_cta + g;
+  long long item = p.spread ? cta * slots_per_cta + (threadIdx.x >> 5) : cta * subs_per_cta + g;
+  if (visitor) {  // the first item from the counter too (the static ones belong to p's own CTAs)
+    long long nxt = 0;
+    if (l == 0 && primary) nxt = n_sw + (long long)atomicAdd(reinterpret_cast<unsigned*>(p.counter), 1u);
+    item = __shfl_sync(kFull, nxt, p.spread ? 0 : leader);
+  }
   bool alive = item < p.n_items;
   long long hyp = 0;
   cx<R> x = mk(R(0), R(0));
@@ -1102,6 +1111,12 @@ __global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const
       if (alive) init_path(item);
     }
   }
+}
+
+template <typename R, typename RL, int N, int W, int KIND, int V, int S, int WK>
+__global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const TrackParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  track_body<R, RL, N, W, KIND, S, WK>(p, smem, blockIdx.x, gridDim.x, false);
 }
 
 // -------------------------------------------------------------------------------------------------

@@ -96,6 +96,7 @@ ghc_kernel_HC_Solver_PH = _sig("ghc_kernel_HC_Solver_PH", ctypes.c_double, _DROP
 ghc_kernel_HC_Solver_PH_z = _sig("ghc_kernel_HC_Solver_PH_z", ctypes.c_double, _DROPIN_PH)
 ghc_measure_fma_peak = _sig("ghc_measure_fma_peak", ctypes.c_int, [ctypes.c_int, _P, _P])
 ghc_lu_solve_device = _sig("ghc_lu_solve_device", ctypes.c_int, [_I32, _I32, _I64, _P, _P, _P, _P])
+ghc_track_mix = _sig("ghc_track_mix", ctypes.c_int, [_P, _P, _I32, _P])
 
 
 class GhcError(RuntimeError):
@@ -246,6 +247,18 @@ def track(pb, ws, d_start_sols, d_coef_hx=None, d_coef_ht=None, d_p_start=None, 
         _check(ghc_track_noalloc(pb.h, ctypes.byref(a), _stream()), "ghc_track_noalloc")
     else:
         _check(ghc_track(pb.h, ctypes.byref(a), _stream()), "ghc_track")
+
+
+def track_mix(buckets):
+    """Batches of different problems in one persistent launch (ghc_track_mix), asynchronous on
+    torch's current stream.  buckets: list of (pb, ws, d_start_sols, kw), kw as for track
+    (plain FP64, no polish).  Bit-identical to calling track for each bucket."""
+    n = len(buckets)
+    pbs = (_P * n)(*[b[0].h for b in buckets])
+    args = (TrackArgs * n)()
+    for i, (pb, ws, ss, kw) in enumerate(buckets):
+        args[i] = _track_args(ws, ss, **kw)
+    _check(ghc_track_mix(ctypes.cast(pbs, _P), ctypes.cast(args, _P), n, _stream()), "ghc_track_mix")
 
 
 def autotune(pb, ws, d_start_sols, **kw):

@@ -211,25 +211,33 @@ def config_mix(args, torch):
         for st in streams:
             main.wait_stream(st)
 
+    def one_launch():
+        ghc.track_mix([(b.pb, b.ws, b.d_sols, dict(b._inputs(), **b.kw)) for b in batches])
+
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    g = _capture(torch, fork_join)
+    g = _capture(torch, one_launch)
     for _ in range(args.warmup):
         g.replay()
     ms = _time_graph(torch, g, args.steps, flush)
+    gf = _capture(torch, fork_join)
+    for _ in range(args.warmup):
+        gf.replay()
+    fork_ms = _time_graph(torch, gf, args.steps, flush)
     # each problem alone, for the overlap benefit
     alone = {}
     for b in batches:
         gb = _capture(torch, b.launch)
         alone[b.name] = statistics.median(_time_graph(torch, gb, 2, flush))
     total_h = sum(h for _, h in MIX)
-    _line("hypothesis-solves/s (uneven mix, one graph launch)", total_h * len(ms) / (sum(ms) * 1e-3), args,
-          {"workload": "uneven mix in one CUDA graph: " + ", ".join("%s %d hyp" % m for m in MIX) +
-                       "; four streams forked and joined inside the graph; FP64, reference step control"},
+    _line("hypothesis-solves/s (uneven mix, one persistent launch)", total_h * len(ms) / (sum(ms) * 1e-3), args,
+          {"workload": "uneven mix in one persistent launch (ghc_track_mix, captured in a CUDA graph): " +
+                       ", ".join("%s %d hyp" % m for m in MIX) + "; FP64, reference step control"},
           ms_per_step=sum(ms) / len(ms), alone_ms=alone, sum_alone_ms=sum(alone.values()),
+          four_streams_in_one_graph_ms=statistics.median(fork_ms),
           tuning=tuning,
           per_problem={b.name: {"hypotheses": b.H, "paths": b.H * b.paths,
                                 "converged_frac": float(b.ws.conv.float().mean())} for b in batches},
-          gpu_launches=8 * args.steps)
+          gpu_launches=4 * args.steps)
 
 
 def config_g3v4_mono(args, torch):

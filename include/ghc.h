@@ -181,6 +181,21 @@ int ghc_track(const ghc_problem* pb, const ghc_track_args* args, void* stream);
 int ghc_track_noalloc(const ghc_problem* pb, const ghc_track_args* args, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Batches of problems of different sizes in one persistent launch (the uneven
+ * mix).  Replaces the reference's one-launch-per-problem dispatch
+ * (GPU-HC/magmaHC/GPU_HC_Solver.cpp:207-349) for a mixed workload: bucket i is
+ * (pbs[i], args[i]) exactly as for ghc_track (its own d_counter; plain FP64, no
+ * polish); CTA ranges start on their own bucket in proportion to its expected
+ * work and move on to the other buckets' counters when it is done, so short
+ * buckets fill the GPU while the long one drains.  Results are bit-identical
+ * to ghc_track launches of the buckets one by one.  Compiled for at most one
+ * bucket each of P2C N = 3, 6, 12 and PH N = 30 with the term shapes of
+ * P3P_TD, 5pt_rel_pos_alg_form_quat, generalized_3views_4pts and
+ * trifocal_2op1p_30x30 (others: GHC_ERR_RANGE).  Asynchronous on `stream`.
+ * ------------------------------------------------------------------------- */
+int ghc_track_mix(const ghc_problem* const* pbs, const ghc_track_args* args, int32_t n_buckets, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Launch tuning.  The reference fixes threads-per-path and block shape per
  * problem in its 21 hand-written wrappers (e.g. kernel_HC_Solver_P3P.cu:284-297:
  * one block of N threads per path); here the sub-warp width follows N and two

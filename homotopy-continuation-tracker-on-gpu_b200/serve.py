@@ -26,6 +26,7 @@ one hypothesis per launch.
 """
 import collections
 import json
+import os
 import time
 
 import numpy as np
@@ -277,8 +278,8 @@ def _stats(lat, hyp, wall):
 
 def bench(args, torch):
     torch.cuda.set_device(0)
-    lams = [100, 300, 1000, 3000, 10000, 20000]
-    n_req = 60
+    lams = [int(v) for v in os.environ.get("GHC_SERVE_LAMBDAS", "100,1000,10000").split(",")]
+    n_req = int(os.environ.get("GHC_SERVE_REQUESTS", "1000"))
     tune = bool(getattr(args, "tune", 1))
     modes = {"batched_fp64": Server(torch, tune=tune),
              "batched_mixed": Server(torch, tune=tune, precision=ghc.PREC_MIXED),

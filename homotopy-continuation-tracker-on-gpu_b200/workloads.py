@@ -3,12 +3,16 @@
 cy       batched: 4096 RANSAC hypotheses of the uncalibrated trifocal problem
          (12 unknowns, 668 paths; seeded 3-camera scenes, minimal samples with
          30 % outlier correspondences) -- device P2C + tracker + FP64 polish
-         captured in one CUDA graph and replayed per step.
+         captured in one CUDA graph and replayed per step: plain FP64 with the
+         reference's step control, then plain FP64 and the mixed tracker (FP32
+         linear algebra, FP64 end game) under the path-jump-free control with
+         the mixed run's recall of the FP64 run's real solutions.
 p3p_td   P3P by a total-degree homotopy: one instance (latency, p50/p99) and
          a batch of 65536 instances (throughput), plain FP64.
-mix      uneven mix in one graph launch: P3P_TD 8192, 5-point 4096,
-         generalized 3-view 2048, trifocal 30x30 1024 hypotheses on four
-         streams forked and joined inside one captured graph.
+mix      uneven mix in one persistent launch (ghc_track_mix): P3P_TD 8192,
+         5-point 4096, generalized 3-view 2048, trifocal 30x30 1024 hypotheses,
+         beside the same four launches forked on four streams of one graph and
+         each bucket alone.
 served   Poisson request stream through serve.Server (continuous batching).
 g3v4_mono  generalized 3-view with start parameters ~ complex N(0,1) and
          start solutions from the monodromy solver, plain FP64 vs mixed.
@@ -147,6 +151,25 @@ def config_cy(args, torch):
         found += best < 1e-6
     steps = b.ws.steps.cpu().numpy()
     total = sum(ms)
+    # the same hypotheses under the path-jump-free control: plain FP64 and the mixed tracker
+    robust = dict(step=ghc.ROBUST_STEP, max_corr=3, max_steps=2000)
+    runs = {}
+    for name, prec in (("fp64", ghc.PREC_FP64), ("mixed", ghc.PREC_MIXED)):
+        r = Batch(torch, "uncalibrated_trifocal_rel_pos_CY", H, 1000 + args.seed, precision=prec, polish=3,
+                  step=robust, scene={"noise_px": 0.0})
+        r_tuning = r.tune() if args.tune else None
+        gr = _capture(torch, r.launch)
+        for _ in range(args.warmup):
+            gr.replay()
+        rms = _time_graph(torch, gr, args.steps, flush)
+        runs[name] = dict(value=H * len(rms) / (sum(rms) * 1e-3), ms=sum(rms) / len(rms), e=_to_cx(r.ws.endpoints),
+                          c=r.ws.conv.cpu().numpy(), r=r.ws.resid.cpu().numpy(), tuning=r_tuning,
+                          steps=float(r.ws.steps.float().mean()))
+    rec, n_real, err = recall_and_error(runs["fp64"], runs["mixed"], b.paths)
+    robust_line = {k: {"value": v["value"], "ms_per_step": v["ms"], "mean_steps": v["steps"], "tuning": v["tuning"]}
+                   for k, v in runs.items()}
+    robust_line["mixed"].update(speedup_vs_fp64=runs["mixed"]["value"] / runs["fp64"]["value"], recall_vs_fp64=rec,
+                                fp64_real_solutions=n_real, endpoint_error_vs_fp64=err)
     _line("hypothesis-solves/s (batched, one graph replay per step)", H * len(ms) / (total * 1e-3), args,
           {"workload": "uncalibrated_trifocal_rel_pos_CY: %d RANSAC hypotheses x 668 paths (%d paths) per step, "
                        "30%% outlier correspondences (inliers exact), FP64, reference step control, FP64 polish, one CUDA graph"
@@ -155,7 +178,30 @@ def config_cy(args, torch):
           paths={"per_step": H * b.paths, "converged_frac": float(conv.mean()), "mean_steps": float(steps.mean()),
                  "max_steps": int(steps.max())},
           inlier_hypotheses=int(inlier.sum()), inlier_ground_truth_found=found / max(1, int(inlier.sum())),
-          tuning=tuning, gpu_launches=3 * args.steps)
+          tuning=tuning, gpu_launches=3 * args.steps,
+          path_jump_free_control={"note": "the same hypotheses, corrector |dx|^2 < 1e-12 |x|^2, first-update test "
+                                          "1e-2, dt <= 0.05, 3 iterations, FP64 polish 3; recall = share of the FP64 "
+                                          "run's real solutions (|Im| <= 1e-8, |H(x,1)| < 1e-10) the mixed run "
+                                          "finds within 1e-8", **robust_line})
+
+
+def recall_and_error(ref, cand, paths):
+    """Share of ref's real solutions (converged, |Im| <= 1e-8, |H(x,1)| < 1e-10) that cand finds within
+    1e-8 (max-norm, relative to max(1, |x|)), hypothesis by hypothesis, with the max and 99th
+    percentile error of the matched endpoints."""
+    e_r, c_r, r_r = ref["e"], ref["c"], ref["r"]
+    real = (c_r == 1) & (np.abs(e_r.imag).max(axis=1) <= 1e-8) & (r_r >= 0) & (r_r < 1e-10)
+    found, errs = 0, []
+    for i in np.nonzero(real)[0]:
+        h = i // paths
+        blk = cand["e"][h * paths:(h + 1) * paths][cand["c"][h * paths:(h + 1) * paths] == 1]
+        d = (np.abs(blk - e_r[i]).max(axis=1) / max(1.0, np.abs(e_r[i]).max())).min() if blk.size else np.inf
+        found += bool(d <= 1e-8)
+        if d <= 1e-8:
+            errs.append(float(d))
+    errs = np.array(errs) if errs else np.zeros(1)
+    return found / max(1, int(real.sum())), int(real.sum()), {"max": float(errs.max()),
+                                                               "p99": float(np.percentile(errs, 99))}
 
 
 def config_p3p_td(args, torch):

@@ -34,21 +34,13 @@ __global__ void __launch_bounds__(128) lu_kernel(long long n_sys, const R* __res
   for (long long s0 = (long long)blockIdx.x * subs; s0 < n_sys; s0 += (long long)gridDim.x * subs) {
     const long long s = s0 + g;
     const bool mine = s < n_sys && l < N;
-    auto load = [&](cx<R>(&row)[N], cx<R>& rhs) {
-      dev::static_for<0, N>([&](auto jc) {
-        constexpr int j = decltype(jc)::value;
-        row[j] = mine ? dev::mk(A[2 * ((s * N + l) * N + j)], A[2 * ((s * N + l) * N + j) + 1]) : dev::mk(R(0), R(0));
-      });
-      rhs = mine ? dev::mk(b[2 * (s * N + l)], b[2 * (s * N + l) + 1]) : dev::mk(R(0), R(0));
-    };
     cx<R> row[N];
-    cx<R> rhs;
-    load(row, rhs);
-    dev::PivotRange<R, false> rg;
-    if (dev::lu_solve<R, N, W>(row, rhs, l, sx, sol, rg)) {
-      load(row, rhs);
-      dev::lu_solve_exact<R, N, W>(row, rhs, l, sx, sol, rg);
-    }
+    dev::static_for<0, N>([&](auto jc) {
+      constexpr int j = decltype(jc)::value;
+      row[j] = mine ? dev::mk(A[2 * ((s * N + l) * N + j)], A[2 * ((s * N + l) * N + j) + 1]) : dev::mk(R(0), R(0));
+    });
+    const cx<R> rhs = mine ? dev::mk(b[2 * (s * N + l)], b[2 * (s * N + l) + 1]) : dev::mk(R(0), R(0));
+    dev::lu_solve<R, N, W>(row, rhs, l, sx, sol);
     if (mine) {
       z[2 * (s * N + l)] = sol[l].re;
       z[2 * (s * N + l) + 1] = sol[l].im;

@@ -413,7 +413,7 @@ struct PivotRange {
 
 template <typename R, int N, int W, bool SPAN>
 __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
-                                                  PivotRange<R, SPAN>& rg, bool& wrong) {
+                                                  PivotRange<R, SPAN>& rg) {
   const bool live = l < N;
   int pos = l;
   static_for<0, N>([&](auto ic) {
@@ -423,15 +423,25 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
     const bool cand = live && pos >= i;
     const unsigned key = live ? pivot_key(m, pos, i) : 0u;
     const unsigned best = pivot_fast<R, W>(key);
-    const int bp = 31 - (int)(best & 31u);
+    int bp = 31 - (int)(best & 31u);
     if (live && pos == bp) {
       static_for<i, N>([&](auto jc) { px[decltype(jc)::value] = A[decltype(jc)::value]; });
       px[N] = b;
     }
     __syncwarp(kFull);
-    const cx<R> p_i = px[i];
-    const R pm = fabs(p_i.re) + fabs(p_i.im);
-    wrong = wrong || cut_was_wrong(m, key, best, cand, pm);
+    cx<R> p_i = px[i];
+    R pm = fabs(p_i.re) + fabs(p_i.im);
+    if (__any_sync(kFull, cut_was_wrong(m, key, best, cand, pm))) {
+      bp = pivot_exact<R, W>(m, cand, pos, i);
+      __syncwarp(kFull);  // every lane has read the first choice
+      if (live && pos == bp) {
+        static_for<i, N>([&](auto jc) { px[decltype(jc)::value] = A[decltype(jc)::value]; });
+        px[N] = b;
+      }
+      __syncwarp(kFull);
+      p_i = px[i];
+      pm = fabs(p_i.re) + fabs(p_i.im);
+    }
     const bool is_piv = live && (pos == bp);
     if (live) {
       if (pos == bp) pos = i;
@@ -474,9 +484,9 @@ __device__ __forceinline__ cx<R> pick(const cx<R> (&A)[N], int i) {
   return a;
 }
 
-template <typename R, int N, int W, bool SPAN, bool EXACT>
+template <typename R, int N, int W, bool SPAN>
 __device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
-                                                PivotRange<R, SPAN>& rg, bool& wrong) {
+                                                PivotRange<R, SPAN>& rg) {
   const bool live = l < N;
   int pos = l;
   cx<R> myrcp = mk(R(0), R(0));
@@ -486,14 +496,8 @@ __device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, c
     const R m = fabs(ai.re) + fabs(ai.im);
     const bool cand = live && pos >= i;
     const unsigned key = live ? pivot_key(m, pos, i) : 0u;
-    unsigned best = 0u;
-    int bp;
-    if constexpr (EXACT) {
-      bp = pivot_exact<R, W>(m, cand, pos, i);
-    } else {
-      best = pivot_fast<R, W>(key);
-      bp = 31 - (int)(best & 31u);
-    }
+    const unsigned best = pivot_fast<R, W>(key);
+    int bp = 31 - (int)(best & 31u);
     if (live && pos == bp) {
 #pragma unroll
       for (int j = 0; j < N; ++j)
@@ -501,9 +505,21 @@ __device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, c
       sx[N] = b;
     }
     __syncwarp(kFull);
-    const cx<R> p_i = sx[i];
-    const R pm = fabs(p_i.re) + fabs(p_i.im);
-    if constexpr (!EXACT) wrong = wrong || cut_was_wrong(m, key, best, cand, pm);
+    cx<R> p_i = sx[i];
+    R pm = fabs(p_i.re) + fabs(p_i.im);
+    if (__any_sync(kFull, cut_was_wrong(m, key, best, cand, pm))) {
+      bp = pivot_exact<R, W>(m, cand, pos, i);
+      __syncwarp(kFull);  // every lane has read the first choice
+      if (live && pos == bp) {
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+          if (j >= i) sx[j] = A[j];
+        sx[N] = b;
+      }
+      __syncwarp(kFull);
+      p_i = sx[i];
+      pm = fabs(p_i.re) + fabs(p_i.im);
+    }
     const bool is_piv = live && (pos == bp);
     if (live) {
       if (pos == bp) pos = i;
@@ -534,24 +550,16 @@ __device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, c
   __syncwarp(kFull);
 }
 
-// The solve with the cut pivot search.  Returns true in every lane of the warp when some lane saw
-// that a column's cut choice was wrong (a near tie of different magnitudes: rare); the caller then
-// solves the original system again with lu_solve_exact -- the same operations in the same order
-// with the exact search, so the result is the reference rule's.
 template <typename R, int N, int W, bool SPAN>
-__device__ __forceinline__ bool lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
+__device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
                                          PivotRange<R, SPAN>& rg) {
-  bool wrong = false;
-  if constexpr (kLuForm<N> == LU_ROLLED) lu_solve_rolled<R, N, W, SPAN, false>(A, b, l, sx, sol, rg, wrong);
-  else lu_solve_unrolled<R, N, W, SPAN>(A, b, l, sx, sol, rg, wrong);
-  return __any_sync(kFull, wrong);
+  if constexpr (kLuForm<N> == LU_ROLLED) lu_solve_rolled<R, N, W>(A, b, l, sx, sol, rg);
+  else lu_solve_unrolled<R, N, W>(A, b, l, sx, sol, rg);
 }
-template <typename R, int N, int W, bool SPAN>
-__device__ __forceinline__ void lu_solve_exact(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
-                                               PivotRange<R, SPAN>& rg) {
-  bool unused = false;
-  rg = PivotRange<R, SPAN>{};
-  lu_solve_rolled<R, N, W, SPAN, true>(A, b, l, sx, sol, rg, unused);
+template <typename R, int N, int W>
+__device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol) {
+  PivotRange<R, false> rg;
+  lu_solve<R, N, W>(A, b, l, sx, sol, rg);
 }
 
 // xor-butterfly sum over the first NP lanes of the sub-warp (order = oracle tree_sum)
@@ -614,19 +622,6 @@ __device__ __forceinline__ void eval_any(const Tables& tb, const SubMem& sm, int
   }
 }
 
-// The rare exact re-solve (a near tie the cut pivot search got wrong): the system evaluated again
-// from shared memory and solved with the exact search.  Out of line and given no register array,
-// so that its registers stay out of the hot path's allocation; the solution lands in sm.sol.
-template <typename R, typename RL, int N, int W, int KIND, int S, bool SPAN>
-__device__ __noinline__ PivotRange<RL, SPAN> exact_resolve(const Tables tb, const SubMem sm, int l, int which) {
-  cx<RL> A[N];
-  cx<RL> b;
-  eval_any<R, RL, N, W, KIND, S>(tb, sm, l, A, b, which);
-  PivotRange<RL, SPAN> rg;
-  lu_solve_exact<RL, N, W>(A, b, l, view<RL>(sm.sx), view<RL>(sm.sol), rg);
-  return rg;
-}
-
 // one evaluation + solve in precision RL; returns this lane's solution component in R.  ill (mixed
 // tracker, cond_limit > 0): the pivot magnitudes spanned more than cond_limit or one was NaN -- the
 // RL solve is too ill-conditioned to keep Newton's contraction
@@ -638,8 +633,7 @@ __device__ __forceinline__ cx<R> eval_solve(const Tables& tb, const SubMem& sm, 
   eval_any<R, RL, N, W, KIND, S>(tb, sm, l, A, b, which);
   constexpr bool kSpan = !std::is_same<R, RL>::value;  // only the mixed tracker tests conditioning
   PivotRange<RL, kSpan> rg;
-  if (lu_solve<RL, N, W>(A, b, l, view<RL>(sm.sx), view<RL>(sm.sol), rg))
-    rg = exact_resolve<R, RL, N, W, KIND, S, kSpan>(tb, sm, l, which);
+  lu_solve<RL, N, W>(A, b, l, view<RL>(sm.sx), view<RL>(sm.sol), rg);
   if constexpr (kSpan) ill = cond_limit > 0.0 && (rg.nan || !(rg.hi <= (RL)cond_limit * rg.lo));
   else ill = false;
   sing = rg.singular();

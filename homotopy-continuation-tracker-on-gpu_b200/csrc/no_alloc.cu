@@ -18,8 +18,9 @@
 //     the rest for the compiled tables; larger problems are rejected with
 //     GHC_ERR_LIMIT and a message naming the sizes.
 //   * set-up: the first call on each device, with that device current, looks
-//     up the array's device address with cudaGetSymbolAddress and caches it;
-//     make that first call before any stream capture.
+//     up the array's device address with cudaGetSymbolAddress and caches it.
+//     The entry point is for eager calls; capture in a CUDA graph is neither
+//     claimed nor tested (a call may copy tables from host memory).
 //   * sharing: all calls on a device use the same array and it keeps the last
 //     call's contents.  A call copies its problem's tables in on the caller's
 //     stream unless the array already holds them (the last call on this device

@@ -278,7 +278,7 @@ def _stats(lat, hyp, wall):
 
 def bench(args, torch):
     torch.cuda.set_device(0)
-    lams = [int(v) for v in os.environ.get("GHC_SERVE_LAMBDAS", "100,1000,10000").split(",")]
+    lams = [int(v) for v in os.environ.get("GHC_SERVE_LAMBDAS", "10,20,40").split(",")]
     n_req = int(os.environ.get("GHC_SERVE_REQUESTS", "1000"))
     tune = bool(getattr(args, "tune", 1))
     modes = {"batched_fp64": Server(torch, tune=tune),
@@ -292,6 +292,8 @@ def bench(args, torch):
         for name, srv in modes.items():
             lat, hyp, wall, _ = run_stream(srv, lam, n_req, seed=lam)
             row["hypotheses"] = hyp
+            # offered load: the stream's hypotheses over its arrival window (n_req / lambda)
+            row["offered_hyp_s"] = hyp * lam / n_req
             row[name] = _stats(lat, hyp, wall)
         rows.append(row)
     dropin = dropin_rate(modes["sequential_fp64"], 64, seed=5)

@@ -171,8 +171,9 @@ int ghc_track(const ghc_problem* pb, const ghc_track_args* args, void* stream);
  * device array of 64 KiB per device, held by every GPU that loads the library
  * until the process exits, and the problem handle itself stays without device
  * memory.  Problems whose compiled tables do not fit return GHC_ERR_LIMIT.  The
- * first call on each device looks up the array's address (make it before any
- * stream capture).  All calls on a device share the array and it keeps the last
+ * first call on each device looks up the array's address.  For eager calls:
+ * nothing is said or tested about capturing it in a CUDA graph (a call may copy
+ * tables from host memory).  All calls on a device share the array and it keeps the last
  * call's contents: a call copies its tables in on `stream` unless the array
  * already holds this handle's tables, and clears the counter on `stream`, so
  * calls ordered on one stream are independent, while calls that overlap on the

@@ -345,8 +345,21 @@ constexpr int kLuForm = N <= 16 ? LU_UNROLLED : GHC_LU_LARGE;
 //                both);
 //   pivot_exact  the full magnitudes and the positions reduced as pairs, run (by the whole warp)
 //                only when some lane saw cut_was_wrong.
+// (one warp-wide redux when the sub-warp is the warp; two sub-warps of 16 reduce at once, the
+// lower half by max over its keys and the upper half by min over its complemented keys; narrower
+// sub-warps by the shuffle butterfly)
 template <typename R, int W>
 __device__ __forceinline__ unsigned pivot_fast(unsigned key) {
+#ifndef GHC_PIVOT_BUTTERFLY
+  if constexpr (W == 32) {
+    return __reduce_max_sync(kFull, key);
+  } else if constexpr (W == 16) {
+    const bool upper = (threadIdx.x & 16u) != 0u;
+    const unsigned lo = __reduce_max_sync(kFull, upper ? 0u : key);
+    const unsigned hi = __reduce_min_sync(kFull, upper ? ~key : ~0u);
+    return upper ? ~hi : lo;
+  }
+#endif
   unsigned best = key;
 #pragma unroll
   for (int off = W / 2; off > 0; off >>= 1) best = max(best, __shfl_xor_sync(kFull, best, off, W));
@@ -807,7 +820,18 @@ __device__ __forceinline__ Tables stage_tables(unsigned char* smem, const uint64
 #ifdef GHC_TRACK_MIN_BLOCKS
 #define GHC_MINB(N, R, RL, V) GHC_TRACK_MIN_BLOCKS
 #else
-#define GHC_MINB(N, R, RL, V) track_min_blocks<N, R, RL, V>()
+#define GHC_MINB(N, R, RL, V) ::ghc::dev::track_min_blocks<N, R, RL, V>()
+#endif
+// Threads per CTA of a tracker instantiation (the launch may still halve it when the per-sub-warp
+// shared memory does not fit).  128 everywhere by default.
+template <int N, typename R, typename RL, int V>
+constexpr int track_block() {
+  return 128;
+}
+#ifdef GHC_TRACK_BLOCK
+#define GHC_BLOCK(N, R, RL, V) GHC_TRACK_BLOCK
+#else
+#define GHC_BLOCK(N, R, RL, V) ::ghc::dev::track_block<N, R, RL, V>()
 #endif
 // WK >= 0: the H_x walk is fixed at compile time (only that walk's code is in the kernel, which
 // spares the register allocator the other walk's read-back: above 16 unknowns, where the row fills
@@ -1117,7 +1141,7 @@ __device__ __forceinline__ void track_body(const TrackParams& p, unsigned char* 
 }
 
 template <typename R, typename RL, int N, int W, int KIND, int V, int S, int WK>
-__global__ void __launch_bounds__(128, GHC_MINB(N, R, RL, V)) track_kernel(const TrackParams p) {
+__global__ void __launch_bounds__(GHC_BLOCK(N, R, RL, V), GHC_MINB(N, R, RL, V)) track_kernel(const TrackParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   track_body<R, RL, N, W, KIND, S, WK>(p, smem, blockIdx.x, gridDim.x, false);
 }

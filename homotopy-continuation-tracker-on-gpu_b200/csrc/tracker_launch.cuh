@@ -15,7 +15,7 @@ constexpr int kBlock = 128;
 // Threads per CTA: 128, or fewer (64, 32) when that many sub-warps' shared memory (per-sub-warp
 // coefficient buffers grow with the problem's coefficient count: 565 complex values x 2 for the
 // generalized 3-view 6-line problem) exceeds what one CTA may use.  0: does not fit at all.
-inline int block_threads(size_t tables, size_t per_sub, int W) {
+inline int block_threads(size_t tables, size_t per_sub, int W, int max_block = kBlock) {
   static int optin = 0;
   if (optin == 0) {
     int dev = 0, v = 0;
@@ -23,7 +23,7 @@ inline int block_threads(size_t tables, size_t per_sub, int W) {
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || v <= 0) v = 48 * 1024;
     optin = v;
   }
-  for (int b = kBlock; b >= 32; b /= 2)
+  for (int b = max_block; b >= 32; b /= 2)
     if (tables + (size_t)(b / W) * per_sub <= (size_t)optin) return b;
   return 0;
 }
@@ -36,7 +36,7 @@ int launch_track_w(const TrackParams& p, cudaStream_t s, int n_sm) {
   const int slots = (dev::kFlatAlways<N> || p.flat_eval) ? p.scr_slots : 0;
   const size_t tables = dev::tables_bytes(N, p.n_hx_terms, p.n_ht_terms);
   const size_t per_sub = dev::sub_bytes(N, Mc, W, slots, 2 * (int)sizeof(RL), 2 * (int)sizeof(R));
-  const int block = block_threads(tables, per_sub, W);
+  const int block = block_threads(tables, per_sub, W, GHC_BLOCK(N, R, RL, V));
   if (block == 0) return -24;
   const int subs = block / W;
   const size_t smem = tables + subs * per_sub;
@@ -143,7 +143,9 @@ int launch_polish_t(const PolishParams& p, cudaStream_t s) {
 }  // namespace launch_detail
 
 
+#ifndef GHC_P2C_SIZES
 #define GHC_P2C_SIZES(X) X(3) X(4) X(5) X(6) X(8) X(10) X(11) X(12) X(16) X(18)
+#endif
 
 // dispatch of one precision mode (state R, linear algebra RL) over the compiled sizes
 template <typename R, typename RL, int V>

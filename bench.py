@@ -70,7 +70,11 @@ def parse():
     ap.add_argument("--hyp", type=int, default=1024)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--quick", action="store_true", help="skip the secondary modes and the CPU baseline")
+    ap.add_argument("--quick", action="store_true", help="skip the secondary modes, the CPU baseline and the other "
+                                                         "workloads' short runs")
+    ap.add_argument("--configs", default="all", choices=["all", "none"],
+                    help="all: append short runs of the other workloads (P3P total degree, CY batch, uneven mix, "
+                         "served stream) to the headline line (one GPU, untimed for the headline)")
     ap.add_argument("--problem", default="trifocal_2op1p_30x30", help="problem folder for --config problem")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "mixed"], help="for --config problem")
     ap.add_argument("--step", default="reference", choices=["reference", "robust"], help="for --config problem")
@@ -376,6 +380,9 @@ def main():
                             "path": "ghc_solve_host (C ABI, pinned host buffers, synchronous, one call per step)"}
             assert np.array_equal(out["conv"], conv), "e2e run differs from the timed run"
             extra["cpu_baseline"] = cpu
+            if args.configs == "all" and world == 1:
+                import workloads
+                extra["configs"] = workloads.summary(args, torch)
     clocks_sum = clocks.summary()
     if dist:
         dist.barrier()
@@ -415,7 +422,7 @@ def main():
         "gpu_launches": 2 * n_steps,
     }
     for k in ("e2e", "cpu_baseline", "oracle_check", "recall_vs_single_hypothesis_fp64", "modes",
-              "dropin_single_hypothesis"):
+              "dropin_single_hypothesis", "configs"):
         if k in extra:
             line[k] = extra[k]
     print(json.dumps(line), flush=True)

@@ -276,10 +276,14 @@ def _stats(lat, hyp, wall):
             "p99_ms": 1e3 * float(np.percentile(lat, 99)), "wall_s": wall}
 
 
-def bench(args, torch):
+def bench(args, torch, lams=None, n_req=None):
+    """The served sweep; returns its JSON line (load points from GHC_SERVE_LAMBDAS or lams, requests
+    per point from GHC_SERVE_REQUESTS or n_req)."""
     torch.cuda.set_device(0)
-    lams = [int(v) for v in os.environ.get("GHC_SERVE_LAMBDAS", "10,20,40").split(",")]
-    n_req = int(os.environ.get("GHC_SERVE_REQUESTS", "1000"))
+    if lams is None:
+        lams = [int(v) for v in os.environ.get("GHC_SERVE_LAMBDAS", "10,20,40").split(",")]
+    if n_req is None:
+        n_req = int(os.environ.get("GHC_SERVE_REQUESTS", "1000"))
     tune = bool(getattr(args, "tune", 1))
     modes = {"batched_fp64": Server(torch, tune=tune),
              "batched_mixed": Server(torch, tune=tune, precision=ghc.PREC_MIXED),
@@ -310,4 +314,4 @@ def bench(args, torch):
             "best_vs_dropin": best / dropin,
             "tuning": {n: p.tuning for n, p in modes["batched_fp64"].problems.items()},
             "sweep": rows}
-    print(json.dumps(line), flush=True)
+    return line

@@ -53,7 +53,7 @@ def _line(metric, value, args, config, **extra):
          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
          "data": "synthetic (seeded scenes)", "config": config}
     d.update(extra)
-    print(json.dumps(d), flush=True)
+    return d
 
 
 class Batch:
@@ -120,8 +120,9 @@ def _capture(torch, fn):
     return g
 
 
-def config_cy(args, torch):
+def config_cy(args, torch, robust_hyp=None):
     H = args.hyp if args.hyp != 1024 else 4096
+    HR = min(H, robust_hyp or H)
     # Inlier correspondences are exact (no pixel noise), so an all-inlier hypothesis has the
     # scene's unknowns as an exact solution and the known answer can be checked at 1e-6.  With
     # 0.5 px noise this minimal problem is so ill-conditioned (focal length from 4 points) that
@@ -155,14 +156,14 @@ def config_cy(args, torch):
     robust = dict(step=ghc.ROBUST_STEP, max_corr=3, max_steps=2000)
     runs = {}
     for name, prec in (("fp64", ghc.PREC_FP64), ("mixed", ghc.PREC_MIXED)):
-        r = Batch(torch, "uncalibrated_trifocal_rel_pos_CY", H, 1000 + args.seed, precision=prec, polish=3,
+        r = Batch(torch, "uncalibrated_trifocal_rel_pos_CY", HR, 1000 + args.seed, precision=prec, polish=3,
                   step=robust, scene={"noise_px": 0.0})
         r_tuning = r.tune() if args.tune else None
         gr = _capture(torch, r.launch)
         for _ in range(args.warmup):
             gr.replay()
         rms = _time_graph(torch, gr, args.steps, flush)
-        runs[name] = dict(value=H * len(rms) / (sum(rms) * 1e-3), ms=sum(rms) / len(rms), e=_to_cx(r.ws.endpoints),
+        runs[name] = dict(value=HR * len(rms) / (sum(rms) * 1e-3), ms=sum(rms) / len(rms), e=_to_cx(r.ws.endpoints),
                           c=r.ws.conv.cpu().numpy(), r=r.ws.resid.cpu().numpy(), tuning=r_tuning,
                           steps=float(r.ws.steps.float().mean()))
     rec, n_real, err = recall_and_error(runs["fp64"], runs["mixed"], b.paths)
@@ -170,7 +171,7 @@ def config_cy(args, torch):
                    for k, v in runs.items()}
     robust_line["mixed"].update(speedup_vs_fp64=runs["mixed"]["value"] / runs["fp64"]["value"], recall_vs_fp64=rec,
                                 fp64_real_solutions=n_real, endpoint_error_vs_fp64=err)
-    _line("hypothesis-solves/s (batched, one graph replay per step)", H * len(ms) / (total * 1e-3), args,
+    return _line("hypothesis-solves/s (batched, one graph replay per step)", H * len(ms) / (total * 1e-3), args,
           {"workload": "uncalibrated_trifocal_rel_pos_CY: %d RANSAC hypotheses x 668 paths (%d paths) per step, "
                        "30%% outlier correspondences (inliers exact), FP64, reference step control, FP64 polish, one CUDA graph"
                        % (H, H * b.paths), "hypotheses_per_step": H, "l2": "flushed before each step"},
@@ -179,7 +180,7 @@ def config_cy(args, torch):
                  "max_steps": int(steps.max())},
           inlier_hypotheses=int(inlier.sum()), inlier_ground_truth_found=found / max(1, int(inlier.sum())),
           tuning=tuning, gpu_launches=3 * args.steps,
-          path_jump_free_control={"note": "the same hypotheses, corrector |dx|^2 < 1e-12 |x|^2, first-update test "
+          path_jump_free_control={"hypotheses": HR, "note": "hypotheses from the same seeded scene generator, corrector |dx|^2 < 1e-12 |x|^2, first-update test "
                                           "1e-2, dt <= 0.05, 3 iterations, FP64 polish 3; recall = share of the FP64 "
                                           "run's real solutions (|Im| <= 1e-8, |H(x,1)| < 1e-10) the mixed run "
                                           "finds within 1e-8", **robust_line})
@@ -228,7 +229,7 @@ def config_p3p_td(args, torch):
     ms = _time_graph(torch, g, args.steps, flush)
     E = _to_cx(batch.ws.endpoints).reshape(H, 8, 3)
     hit = np.mean([np.abs(E[h] - batch.truth[h]).max(axis=1).min() < 1e-9 for h in range(0, H, 64)])
-    _line("hypothesis-solves/s (P3P total degree)", H * len(ms) / (sum(ms) * 1e-3), args,
+    return _line("hypothesis-solves/s (P3P total degree)", H * len(ms) / (sum(ms) * 1e-3), args,
           {"workload": "P3P_TD: 3 depths, 8 total-degree paths, seeded unit-modulus gamma; 1 instance (latency) "
                        "and %d instances per step (throughput); FP64 with polish" % H},
           ms_per_step=sum(ms) / len(ms), single_instance={"p50_ms": float(np.percentile(lat, 50)),
@@ -275,7 +276,7 @@ def config_mix(args, torch):
         gb = _capture(torch, b.launch)
         alone[b.name] = statistics.median(_time_graph(torch, gb, 2, flush))
     total_h = sum(h for _, h in MIX)
-    _line("hypothesis-solves/s (uneven mix, one persistent launch)", total_h * len(ms) / (sum(ms) * 1e-3), args,
+    return _line("hypothesis-solves/s (uneven mix, one persistent launch)", total_h * len(ms) / (sum(ms) * 1e-3), args,
           {"workload": "uneven mix in one persistent launch (ghc_track_mix, captured in a CUDA graph): " +
                        ", ".join("%s %d hyp" % m for m in MIX) + "; FP64, reference step control"},
           ms_per_step=sum(ms) / len(ms), alone_ms=alone, sum_alone_ms=sum(alone.values()),
@@ -323,7 +324,7 @@ def config_g3v4_mono(args, torch):
             found += bool(d.size and d.min() <= 1e-8)
         E = e64[h][c64[h]]
         gt_hits += bool(E.size and (np.abs(E - truth[h]).max(axis=1) / np.abs(truth[h]).max()).min() < 1e-6)
-    _line("hypothesis-solves/s at real-sol recall, mixed vs plain FP64 (own start system)", out["mixed"]["value"],
+    return _line("hypothesis-solves/s at real-sol recall, mixed vs plain FP64 (own start system)", out["mixed"]["value"],
           args, {"workload": "generalized_3views_4pts: start params ~ complex N(0,1) (seed %d), %d start solutions "
                              "from the monodromy solver, %d seeded exact scenes per step, path-jump-free "
                              "step control, FP64 polish" % (args.seed, len(Sq), H)},
@@ -347,7 +348,7 @@ def config_problem(args, torch):
     steps = b.ws.steps.cpu().numpy().astype(np.int64)
     solves = 4 * steps + b.ws.corr.cpu().numpy()
     total = sum(ms)
-    _line("hypothesis-solves/s (one problem, batched)", H * len(ms) / (total * 1e-3), args,
+    return _line("hypothesis-solves/s (one problem, batched)", H * len(ms) / (total * 1e-3), args,
           {"workload": "%s: %d hypotheses x %d paths per launch, %s, %s step control, one CUDA graph"
                        % (args.problem, H, b.paths, args.precision, args.step), "l2": "flushed before each step"},
           ms_per_step=total / len(ms), p50_ms=float(np.percentile(ms, 50)),
@@ -403,7 +404,7 @@ def config_latency(args, torch):
         ratios.append(row["fp32_speedup_vs_published"])
         out[name] = row
     gm = float(np.exp(np.mean(np.log(ratios))))
-    _line("single-instance latency vs the reference's published times (geometric mean of ratios, FP32)", gm, args,
+    return _line("single-instance latency vs the reference's published times (geometric mean of ratios, FP32)", gm, args,
           {"workload": "one instance per launch: the shipped start/target parameters of P3P, 5-point, "
                        "generalized 3-view, uncalibrated trifocal CY and trifocal 30x30; reference step control; "
                        "p50 over %d launches each" % n},
@@ -411,13 +412,33 @@ def config_latency(args, torch):
           gpu_launches=launches)
 
 
-def config_served(args, torch):
+def config_served(args, torch, lams=None, n_req=None):
     import serve
-    serve.bench(args, torch)
+    return serve.bench(args, torch, lams=lams, n_req=n_req)
 
 
 def run(args):
     import torch
     torch.cuda.set_device(0)
-    {"cy": config_cy, "p3p_td": config_p3p_td, "mix": config_mix, "served": config_served,
-     "g3v4_mono": config_g3v4_mono, "problem": config_problem, "latency": config_latency}[args.config](args, torch)
+    line = {"cy": config_cy, "p3p_td": config_p3p_td, "mix": config_mix, "served": config_served,
+            "g3v4_mono": config_g3v4_mono, "problem": config_problem,
+            "latency": config_latency}[args.config](args, torch)
+    print(json.dumps(line), flush=True)
+
+
+def summary(args, torch):
+    """Short runs of the other configured workloads, for the headline bench line: P3P by total
+    degree (config 1), CY RANSAC batch (config 3; the path-jump-free comparison on its first 512
+    hypotheses), the uneven mix (config 4) and the served stream (config 5: one load point of 200
+    requests).  Each entry is that workload's own line."""
+    import argparse
+    short = argparse.Namespace(**vars(args))
+    short.steps, short.warmup, short.hyp = 2, 1, 1024
+    out = {}
+    for name, fn, kw in (("p3p_td", config_p3p_td, {}), ("cy", config_cy, {"robust_hyp": 512}),
+                         ("mix", config_mix, {}), ("served", config_served, {"lams": [20], "n_req": 200})):
+        t0 = time.time()
+        line = fn(short, torch, **kw)
+        line["wall_s"] = time.time() - t0
+        out[name] = line
+    return out

@@ -336,7 +336,8 @@ constexpr int kLuForm = N <= 16 ? LU_UNROLLED : GHC_LU_LARGE;
 
 // Pivot position of column i by the reference's rule (dev-cgesv-batched-small.cuh:54-65): the
 // largest |Re|+|Im| among the unpivoted rows, the lowest position among equal magnitudes, a NaN at
-// position i kept and a NaN below never taken.  Two steps:
+// position i kept and a NaN below never taken.  Sub-warps of 16 and 32 lanes: pivot_redux3 (below),
+// exact in three warp reductions.  Narrower sub-warps, two steps:
 //   pivot_fast   an integer max butterfly over pivot_key (one shuffle per level): the largest cut
 //                magnitude, the lowest position among equal cut magnitudes;
 //   cut_was_wrong  after the chosen row is broadcast, true on a lane whose row shares the winner's
@@ -345,21 +346,8 @@ constexpr int kLuForm = N <= 16 ? LU_UNROLLED : GHC_LU_LARGE;
 //                both);
 //   pivot_exact  the full magnitudes and the positions reduced as pairs, run (by the whole warp)
 //                only when some lane saw cut_was_wrong.
-// (one warp-wide redux when the sub-warp is the warp; two sub-warps of 16 reduce at once, the
-// lower half by max over its keys and the upper half by min over its complemented keys; narrower
-// sub-warps by the shuffle butterfly)
 template <typename R, int W>
 __device__ __forceinline__ unsigned pivot_fast(unsigned key) {
-#ifndef GHC_PIVOT_BUTTERFLY
-  if constexpr (W == 32) {
-    return __reduce_max_sync(kFull, key);
-  } else if constexpr (W == 16) {
-    const bool upper = (threadIdx.x & 16u) != 0u;
-    const unsigned lo = __reduce_max_sync(kFull, upper ? 0u : key);
-    const unsigned hi = __reduce_min_sync(kFull, upper ? ~key : ~0u);
-    return upper ? ~hi : lo;
-  }
-#endif
   unsigned best = key;
 #pragma unroll
   for (int off = W / 2; off > 0; off >>= 1) best = max(best, __shfl_xor_sync(kFull, best, off, W));
@@ -399,6 +387,57 @@ __device__ __forceinline__ int pivot_exact(R m, bool cand, int pos, int i) {
   return mp;
 }
 
+// Warp reductions of the sub-warp (W = 16 or 32): max and min of a 32-bit value over the
+// sub-warp's lanes; two sub-warps of 16 reduce at once, one by the operation, the other by the
+// opposite operation on complemented values.
+template <int W>
+__device__ __forceinline__ unsigned subwarp_max(unsigned v) {
+  static_assert(W == 16 || W == 32, "redux reductions need a sub-warp of 16 or 32");
+  if constexpr (W == 32) {
+    return __reduce_max_sync(kFull, v);
+  } else {
+    const bool upper = (threadIdx.x & 16u) != 0u;
+    const unsigned lo = __reduce_max_sync(kFull, upper ? 0u : v);
+    const unsigned hi = __reduce_min_sync(kFull, upper ? ~v : ~0u);
+    return upper ? ~hi : lo;
+  }
+}
+template <int W>
+__device__ __forceinline__ unsigned subwarp_min(unsigned v) {
+  static_assert(W == 16 || W == 32, "redux reductions need a sub-warp of 16 or 32");
+  if constexpr (W == 32) {
+    return __reduce_min_sync(kFull, v);
+  } else {
+    const bool upper = (threadIdx.x & 16u) != 0u;
+    const unsigned lo = __reduce_min_sync(kFull, upper ? ~0u : v);
+    const unsigned hi = __reduce_max_sync(kFull, upper ? ~v : 0u);
+    return upper ? ~hi : lo;
+  }
+}
+// The exact pivot position of column i in three sub-warp reductions (sub-warps of 16 or 32):
+// the largest upper word of the candidates' magnitudes (shifted up by one so that a candidate
+// with magnitude 0 still outranks a non-candidate; a NaN at position i above everything, a NaN
+// below excluded), then the largest lower word among the candidates with that upper word, then
+// the lowest position among those with both -- the reference's strict-> scan in position order.
+// The candidate at position i always takes part, so some lane always wins.
+template <typename R, int W>
+__device__ __forceinline__ int pivot_redux3(R m, bool cand, int pos, int i) {
+  const unsigned long long mb = full_bits(m);
+  const unsigned hi = sizeof(R) == 8 ? (unsigned)(mb >> 32) : (unsigned)mb;
+  unsigned khi = 0u;
+  if (cand) khi = (m == m) ? hi + 1u : (pos == i ? 0xffffffffu : 0u);
+  const unsigned top = subwarp_max<W>(khi);
+  bool win = khi != 0u && khi == top;
+  if constexpr (sizeof(R) == 8) {
+    const unsigned lo = (unsigned)mb;
+    const unsigned low = subwarp_max<W>(win ? lo : 0u);
+    win = win && lo == low;
+  }
+  return (int)subwarp_min<W>(win ? (unsigned)pos : 63u);
+}
+template <int W>
+constexpr bool kPivotRedux3 = W == 16 || W == 32;
+
 // PivotRange: what one solve saw of its pivot magnitudes |U_ii| (|Re|+|Im|), in the oracle's
 // comparison order.  singular(): a zero pivot, unless column 0's magnitude was NaN (the oracle's
 // running minimum then stays NaN).  With SPAN (the mixed tracker's conditioning test) also the
@@ -434,9 +473,15 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
     cx<R>* px = sx + (i & 1) * (N + 1);
     const R m = fabs(A[i].re) + fabs(A[i].im);
     const bool cand = live && pos >= i;
-    const unsigned key = live ? pivot_key(m, pos, i) : 0u;
-    const unsigned best = pivot_fast<R, W>(key);
-    int bp = 31 - (int)(best & 31u);
+    int bp;
+    unsigned key = 0u, best = 0u;
+    if constexpr (kPivotRedux3<W>) {
+      bp = pivot_redux3<R, W>(m, cand, pos, i);
+    } else {
+      key = live ? pivot_key(m, pos, i) : 0u;
+      best = pivot_fast<R, W>(key);
+      bp = 31 - (int)(best & 31u);
+    }
     if (live && pos == bp) {
       static_for<i, N>([&](auto jc) { px[decltype(jc)::value] = A[decltype(jc)::value]; });
       px[N] = b;
@@ -444,7 +489,7 @@ __device__ __forceinline__ void lu_solve_unrolled(cx<R> (&A)[N], cx<R> b, int l,
     __syncwarp(kFull);
     cx<R> p_i = px[i];
     R pm = fabs(p_i.re) + fabs(p_i.im);
-    if (__any_sync(kFull, cut_was_wrong(m, key, best, cand, pm))) {
+    if (!kPivotRedux3<W> && __any_sync(kFull, cut_was_wrong(m, key, best, cand, pm))) {
       bp = pivot_exact<R, W>(m, cand, pos, i);
       __syncwarp(kFull);  // every lane has read the first choice
       if (live && pos == bp) {

@@ -91,3 +91,23 @@ def test_monodromy_finds_all_p3p_solutions():
     pb = ghc.Problem("P3P")
     q, Sq, S = monodromy.start_system(pb, seed=3)
     assert len(S) == 8 and len(Sq) == 8
+
+
+def test_admission_waits_for_free_memory():
+    """With the device reporting too little free memory, batches wait in the queue (in order) and
+    start once memory frees up; results are those of an unconstrained server."""
+    calls = {"n": 0}
+
+    def scarce():
+        calls["n"] += 1
+        free, total = torch.cuda.mem_get_info()
+        return (0 if 2 <= calls["n"] <= 40 else free), total  # the first call sizes the slots
+
+    tight = serve.Server(torch, problems=["P3P_TD"], max_batch=512, mem_info=scarce)
+    free = serve.Server(torch, problems=["P3P_TD"], max_batch=512)
+    _, _, _, rt = serve.run_stream(tight, lam=5000, n_req=6, seed=21)
+    _, _, _, rf = serve.run_stream(free, lam=5000, n_req=6, seed=21)
+    assert tight.deferred > 0 and free.deferred == 0
+    for x, y in zip(rt, rf):
+        assert x.done is not None
+        assert np.array_equal(x.endpoints, y.endpoints) and np.array_equal(x.counts, y.counts)

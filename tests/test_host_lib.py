@@ -213,3 +213,13 @@ def test_no_alloc_rejects_tables_beyond_its_fixed_array(tmp_path):
     msg = ghc.ghc_last_error().decode()
     assert "65536" in msg and "ghc_track" in msg
     assert pb.bound_device() == -1
+
+
+def test_serve_admission_rule():
+    """Live admission: a batch starts only if its transient coefficient tables leave the reserve free."""
+    import serve
+    pb = ghc.Problem("generalized_3views_4pts")
+    need = serve.transient_bytes(pb, 100)
+    assert need == 16 * 100 * (pb.M + 1) * (2 * pb.K + 1)
+    assert serve.transient_bytes(ghc.Problem("trifocal_2op1p_30x30"), 100) == 0  # PH: slot buffers only
+    assert serve.admit(need + 1000, need, 1000) and not serve.admit(need + 999, need, 1000)

@@ -28,9 +28,9 @@ __global__ void __launch_bounds__(128) lu_kernel(long long n_sys, const R* __res
   const int l = lane % W;
   const int g = threadIdx.x / W;
   const int subs = blockDim.x / W;
-  // per sub-warp: two pivot rows + right-hand side [2 (N+1)], solution [N]
-  cx<R>* sx = dev::view<R>(smem) + (size_t)g * (3 * N + 2);
-  cx<R>* sol = sx + 2 * (N + 1);
+  // per sub-warp: the solve scratch [lu_scratch_len(N)] (pivot rows, or the whole system), solution [N]
+  cx<R>* sx = dev::view<R>(smem) + (size_t)g * (dev::lu_scratch_len(N) + N);
+  cx<R>* sol = sx + dev::lu_scratch_len(N);
   for (long long s0 = (long long)blockIdx.x * subs; s0 < n_sys; s0 += (long long)gridDim.x * subs) {
     const long long s = s0 + g;
     const bool mine = s < n_sys && l < N;
@@ -53,7 +53,7 @@ template <typename R, int N>
 int launch_lu(long long n_sys, const void* A, const void* b, void* z, cudaStream_t s) {
   constexpr int W = subwarp_width(N);
   const int subs = 128 / W;
-  const size_t smem = (size_t)subs * (3 * N + 2) * sizeof(cx<R>);
+  const size_t smem = (size_t)subs * (dev::lu_scratch_len(N) + N) * sizeof(cx<R>);
   long long grid = (n_sys + subs - 1) / subs;
   if (grid > 148LL * 16) grid = 148LL * 16;
   lu_kernel<R, N, W><<<(unsigned)grid, 128, smem, s>>>(n_sys, (const R*)A, (const R*)b, (R*)z);

@@ -327,12 +327,25 @@ __device__ __forceinline__ void static_for(F&& f) {
 //                predicated on j > i (N^2 instead of N^2/2 issue slots, code
 //                linear in N).
 // pragma unroll alone gives up above N = 16 and moves the row to local memory.
-constexpr int LU_UNROLLED = 0, LU_ROLLED = 1;
+//   LU_SERIAL    (N <= 3) every lane of the sub-warp gathers the whole system
+//                through shared memory and eliminates it in its registers, rows
+//                swapped by selects: no pivot search across lanes and no
+//                broadcast per column, so a lone small system's solve is a short
+//                chain (the single-instance P3P case is latency bound).
+constexpr int LU_UNROLLED = 0, LU_ROLLED = 1, LU_SERIAL = 2;
 #ifndef GHC_LU_LARGE
 #define GHC_LU_LARGE LU_UNROLLED
 #endif
+#ifndef GHC_LU_SERIAL_MAX_N
+#define GHC_LU_SERIAL_MAX_N 3
+#endif
 template <int N>
-constexpr int kLuForm = N <= 16 ? LU_UNROLLED : GHC_LU_LARGE;
+constexpr int kLuForm = N <= GHC_LU_SERIAL_MAX_N ? LU_SERIAL : N <= 16 ? LU_UNROLLED : GHC_LU_LARGE;
+// complex values of the per-sub-warp solve scratch sx: two pivot rows with their right-hand sides,
+// or, for the serial form, the whole system
+__host__ __device__ inline int lu_scratch_len(int N) {
+  return N <= GHC_LU_SERIAL_MAX_N ? N * (N + 1) : 2 * (N + 1);
+}
 
 // Pivot position of column i by the reference's rule (dev-cgesv-batched-small.cuh:54-65): the
 // largest |Re|+|Im| among the unpivoted rows, the lowest position among equal magnitudes, a NaN at
@@ -608,10 +621,84 @@ __device__ __forceinline__ void lu_solve_rolled(cx<R> (&A)[N], cx<R> b, int l, c
   __syncwarp(kFull);
 }
 
+// The serial form: the oracle's elimination (rows at positions, strict-> scan from position i,
+// zero pivot skipping its column, back substitution by the stored reciprocals) run by every lane
+// on its own copy of the system; lane l leaves component l of the solution in sol[l].
+template <typename R, int N, int W, bool SPAN>
+__device__ __forceinline__ void lu_solve_serial(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
+                                                PivotRange<R, SPAN>& rg) {
+  constexpr int C = N + 1;  // row length with the right-hand side
+  if (l < N) {
+    static_for<0, N>([&](auto jc) { sx[l * C + decltype(jc)::value] = A[decltype(jc)::value]; });
+    sx[l * C + N] = b;
+  }
+  __syncwarp(kFull);
+  cx<R> M[N][C];
+  static_for<0, N>([&](auto rc_) {
+    static_for<0, C>([&](auto jc) { M[decltype(rc_)::value][decltype(jc)::value] = sx[decltype(rc_)::value * C + decltype(jc)::value]; });
+  });
+  __syncwarp(kFull);  // every lane has its copy before the next solve rewrites sx
+  cx<R> rcp[N];
+  static_for<0, N>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    R best = fabs(M[i][i].re) + fabs(M[i][i].im);
+    int bp = i;
+    static_for<i + 1, N>([&](auto jc) {
+      constexpr int j = decltype(jc)::value;
+      const R v = fabs(M[j][i].re) + fabs(M[j][i].im);
+      if (v > best) {
+        best = v;
+        bp = j;
+      }
+    });
+    rg.add(i, best);
+    // the pivot row moves to position i, the row at position i to the pivot's position
+    static_for<i + 1, N>([&](auto jc) {
+      constexpr int j = decltype(jc)::value;
+      if (bp == j) {
+        static_for<i, C>([&](auto kc) {
+          constexpr int k = decltype(kc)::value;
+          const cx<R> t = M[i][k];
+          M[i][k] = M[j][k];
+          M[j][k] = t;
+        });
+      }
+    });
+    const bool zero = best == R(0);
+    rcp[i] = c_rcp(M[i][i]);
+    if (!zero) {
+      static_for<i + 1, N>([&](auto rc_) {
+        constexpr int r = decltype(rc_)::value;
+        M[r][i] = c_mul(M[r][i], rcp[i]);
+        static_for<i + 1, C>([&](auto jc) {
+          constexpr int j = decltype(jc)::value;
+          M[r][j] = c_fnma(M[r][i], M[i][j], M[r][j]);
+        });
+      });
+    }
+  });
+  cx<R> z[N];
+  static_for<0, N>([&](auto ic) {
+    constexpr int i = N - 1 - decltype(ic)::value;
+    z[i] = c_mul(M[i][N], rcp[i]);
+    static_for<0, i>([&](auto rc_) {
+      constexpr int r = decltype(rc_)::value;
+      M[r][N] = c_fnma(M[r][i], z[i], M[r][N]);
+    });
+  });
+  cx<R> mine = z[0];
+  static_for<1, N>([&](auto jc) {
+    if (l == decltype(jc)::value) mine = z[decltype(jc)::value];
+  });
+  if (l < N) sol[l] = mine;
+  __syncwarp(kFull);
+}
+
 template <typename R, int N, int W, bool SPAN>
 __device__ __forceinline__ void lu_solve(cx<R> (&A)[N], cx<R> b, int l, cx<R>* sx, cx<R>* sol,
                                          PivotRange<R, SPAN>& rg) {
-  if constexpr (kLuForm<N> == LU_ROLLED) lu_solve_rolled<R, N, W>(A, b, l, sx, sol, rg);
+  if constexpr (kLuForm<N> == LU_SERIAL) lu_solve_serial<R, N, W>(A, b, l, sx, sol, rg);
+  else if constexpr (kLuForm<N> == LU_ROLLED) lu_solve_rolled<R, N, W>(A, b, l, sx, sol, rg);
   else lu_solve_unrolled<R, N, W>(A, b, l, sx, sol, rg);
 }
 template <typename R, int N, int W>
@@ -635,7 +722,7 @@ struct SubMem {
   unsigned char* coefA;  // c_k(t)   or p(t)     [Mc]
   unsigned char* coefB;  // c'_k(t)  or p1 - p0  [Mc]
   unsigned char* xs;     // track [N+1]
-  unsigned char* sx;     // two pivot rows + rhs [2][N+1]
+  unsigned char* sx;     // solve scratch [lu_scratch_len(N)]: two pivot rows + rhs, or the whole system
   unsigned char* sol;    // solution [N]
   unsigned char* state;  // per lane: RK base point x0 [W], RK accumulator [W] (state precision)
   unsigned char* scr;    // H_x row scratch [slots][W], null unless the evaluation is flat
@@ -735,7 +822,7 @@ __host__ __device__ inline size_t tables_bytes(int N, int n_hx, int n_ht) {
   return align16(8 * (size_t)(n_hx + n_ht) + 2 * (size_t)(hx_off_len(N) + N + 1));
 }
 // Per sub-warp: the path record [kRecBytes], then, in complex values of e bytes (linear-algebra
-// precision): coefficient buffers [2 Mc], track [N+1], two pivot rows [2 (N+1)], solution [N]; the
+// precision): coefficient buffers [2 Mc], track [N+1], solve scratch [lu_scratch_len(N)], solution [N]; the
 // lane state [2 W] in complex values of es bytes (state precision); scratch slots [slots W] (flat);
 // and, when es != e (mixed), the state-precision coefficients [Mc] and track [N+1].
 struct SubOffsets {
@@ -752,7 +839,7 @@ __host__ __device__ inline SubOffsets sub_offsets(int N, int Mc, int W, int slot
   o.xs = off;
   off += (size_t)e * (N + 1);
   o.sx = off;
-  off += (size_t)e * 2 * (N + 1);
+  off += (size_t)e * lu_scratch_len(N);
   o.sol = off;
   off += (size_t)e * N;
   if (mixed) off = align16(off);

@@ -85,14 +85,17 @@ int launch_track_w(const TrackParams& p, cudaStream_t s, int n_sm) {
   return e == cudaSuccess ? 0 : -23;
 }
 
-// above 16 unknowns one kernel per H_x walk (row-wise, balanced), else the walk is chosen at run time
+// one kernel per H_x walk (entry-wise, row-wise, balanced where built; above 16 unknowns never entry-wise)
 template <typename R, typename RL, int N, int KIND, int V, int S>
 int launch_track_s(const TrackParams& p, cudaStream_t s, int n_sm) {
   if constexpr (N > 16) {
     if (p.flat_eval == 2 && balanced_walk_built(N)) return launch_track_w<R, RL, N, KIND, V, S, 2>(p, s, n_sm);
     return launch_track_w<R, RL, N, KIND, V, S, 1>(p, s, n_sm);
   } else {
-    return launch_track_w<R, RL, N, KIND, V, S, -1>(p, s, n_sm);
+    // one kernel per walk here too: only the chosen walk's code is in the loop body
+    if (p.flat_eval == 2 && balanced_walk_built(N)) return launch_track_w<R, RL, N, KIND, V, S, 2>(p, s, n_sm);
+    if (p.flat_eval != 0) return launch_track_w<R, RL, N, KIND, V, S, 1>(p, s, n_sm);
+    return launch_track_w<R, RL, N, KIND, V, S, 0>(p, s, n_sm);
   }
 }
 

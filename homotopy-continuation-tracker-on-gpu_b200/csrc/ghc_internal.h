@@ -53,10 +53,11 @@ constexpr int kMaxVarsBalanced = 5;
 // lanes per path (the sub-warp width) for N unknowns
 GHC_HD constexpr int subwarp_width(int N) { return N <= 4 ? 4 : N <= 8 ? 8 : N <= 16 ? 16 : 32; }
 
-// Sizes that get the balanced H_x walk (tables and kernel code).  B200, tuned: 5-point (N = 6)
-// +11 %, 30x30 (N = 30) +4 %; at N = 12 both shipped problems ran 4-5 % slower even on the
-// row-wise walk once the balanced code and its tables were in the kernel, so it is left out there.
-GHC_HD constexpr bool balanced_walk_built(int N) { return N <= 8 || N > 16; }
+// Sizes that get the balanced H_x walk (tables and kernel code): every size.  B200, tuned: 5-point
+// (N = 6) +11 %, 30x30 (N = 30) +4 %.  (When the walk was chosen at run time inside one kernel, the
+// balanced code cost the N = 12 problems 4-5 % on their row-wise walk; each walk is its own kernel
+// now, so building it costs the other walks nothing.)
+GHC_HD constexpr bool balanced_walk_built(int) { return true; }
 
 // The compiled H_x offsets: [N*N+1] CSR offsets of the terms per (row, column), then the
 // balanced walk: [1] its first word in the term array (kNoLanes: no balanced walk) and

@@ -5,7 +5,7 @@ dev-eval-indxing-P3P.cuh:70-84 reads it term by term) appears once, in table ord
 scale, coefficient (or parameter pair), every variable slot including the constant slot N, its
 column and the last-term-of-entry flag.  Balanced block: every entry's terms are walked by one
 lane, in the same order, and stored to the entry's row and slot; the lanes' lengths are what the
-walk runs, and sizes without the balanced walk carry none.
+walk runs.
 """
 import numpy as np
 import pytest
@@ -75,10 +75,7 @@ def test_balanced_block_walks_every_entry_once_in_order(name):
     words, off = pb.compiled_hx()
     first = int(off[N * N + 1])
     lens = [int(x) for x in off[N * N + 2:]]
-    if N > 8 and N <= 16:
-        assert first == 0xFFFF and sum(lens) == 0  # not built at these sizes
-        return
-    assert first != 0xFFFF
+    assert first != 0xFFFF  # built at every size
     assert sum(lens) == int(off[N * N])
     want = {}
     for r in range(N):
@@ -109,4 +106,6 @@ def test_sizes_and_errors():
     pb = ghc.Problem("generalized_3views_4pts")
     w, o = pb.compiled_hx()
     assert int(o[pb.N * pb.N]) == pb.info.n_hx_terms == 144
-    assert len(w) == 12 * 12  # row block only at N = 12
+    lens = [int(x) for x in o[pb.N * pb.N + 2:]]
+    assert len(w) == 12 * 12 + 16 * max(lens)  # row block (12 rows x 12 terms), then the balanced block
+    assert max(lens) == 9  # the 144 terms dealt to 16 lanes

@@ -59,7 +59,7 @@ def test_autotune_keeps_a_candidate():
     pb, ob, tg = _inputs("generalized_3views_4pts", H=8)
     ref, _ = _run(pb, ob, tg, ghc.PREC_FP64, (0, -1))
     ws, choice = _run(pb, ob, tg, ghc.PREC_FP64, "auto")
-    assert choice["candidates"] == 4 and choice["ms"] > 0  # 2 register budgets x 2 H_x walks (no balanced walk at N = 12)
+    assert choice["candidates"] == 6 and choice["ms"] > 0  # 2 register budgets x 3 H_x walks
     assert ghc.get_tuning(pb, ghc.PREC_FP64) == (choice["variant"], choice["flat"])
     assert torch.equal(ws.endpoints, ref.endpoints)  # the sample's outputs are a regular run's
     again, _ = _run(pb, ob, tg, ghc.PREC_FP64)
@@ -67,11 +67,11 @@ def test_autotune_keeps_a_candidate():
 
 
 def test_mixed_autotune_chooses_each_phase():
-    """Mixed precision tunes the FP64 and FP32 phases' variants independently (2 x 2 x 2 walks at N = 12)."""
+    """Mixed precision tunes the FP64 and FP32 phases' variants independently (2 x 2 x 3 walks at N = 12)."""
     pb, ob, tg = _inputs("generalized_3views_4pts", H=8)
     ref, _ = _run(pb, ob, tg, ghc.PREC_MIXED, (0, -1))
     ws, choice = _run(pb, ob, tg, ghc.PREC_MIXED, "auto")
-    assert choice["candidates"] == 8
+    assert choice["candidates"] == 12
     assert ghc.get_tuning(pb, ghc.PREC_FP64) == (choice["variant"], choice["flat"])
     assert ghc.get_tuning(pb, ghc.PREC_FP32) == (choice["variant_f32"], choice["flat"])
     assert torch.equal(ws.endpoints, ref.endpoints)
